@@ -1,0 +1,939 @@
+// ocfd_api.cu -- the C ABI of include/ocfd_gpu.h: instance lifetime, device
+// buffers, the stage operators of NS_solver, the fused graph-captured step,
+// diagnostics and the batched ensemble.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "ocfd_gpu.h"
+#include "ocfd_kernels.h"
+
+using namespace ocfd;
+
+struct ocfd_handle {
+  ocfd_params p;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  Grid g;
+  Phys ph;
+  DCoef dc;
+  bool mixed = false;
+  bool chr = false;
+  bool fuse_bc = false;
+  // state
+  double* f = nullptr;
+  double* fn = nullptr;
+  double* du = nullptr;
+  double* prim[5] = {};
+  double* talt = nullptr;  // second temperature buffer (negative-T repair)
+  float* p32[5] = {};
+  double* met[OCFD_N_METRICS] = {};
+  float* met32[OCFD_N_METRICS] = {};
+  double* rh = nullptr;
+  void* hf[3] = {};
+  long long fs[3] = {};
+  void* ev = nullptr;
+  double* scratch = nullptr;
+  size_t scratch_n = 0;
+  DevStatus* dstat = nullptr;
+  DevStatus* hstat = nullptr;  // pinned
+  double* dout = nullptr;      // small device output block
+  double* hout = nullptr;      // pinned
+  double** dptr = nullptr;     // device pointer table (halo lists)
+  // graphs: one step, for each parity of the (f,fn) and T buffer pairs
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int parity = 0;
+  bool halo_valid = false;
+  bool metrics_ready = false;
+  int istep = 0;
+  double tt = 0.0;
+  std::string err;
+  std::vector<double> pmask;  // unused, keeps layout stable
+};
+
+namespace {
+
+int fail(ocfd_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+int cuda_fail(ocfd_handle* h, cudaError_t e, const char* where) {
+  return fail(h, OCFD_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e__ = (call);                           \
+    if (e__ != cudaSuccess) return cuda_fail(h, e__, #call); \
+  } while (0)
+
+// ------------------------------------------------------------------ params
+void fill_phys(const ocfd_params& p, Phys& ph, DCoef& dc) {
+  memset(&ph, 0, sizeof(ph));
+  ph.gamma = p.gamma;
+  ph.ma = p.ma;
+  ph.re = p.re;
+  ph.pr = p.pr;
+  ph.cv = p.cv;
+  ph.cp = p.cp;
+  ph.dt = p.dt;
+  ph.ref_amu_t0 = p.ref_amu_t0;
+  ph.hx = p.hx;
+  ph.hy = p.hy;
+  ph.hz = p.hz;
+  for (int q = 0; q < 8; q++) ph.ud7l[q] = p.ud7l[q];
+  ph.hyb1 = p.hybrid_para[1];
+  ph.hyb2 = p.hybrid_para[2];
+  for (int q = 0; q < 3; q++) ph.mass_force[q] = p.mass_force[q];
+  ph.if_mass_force = p.if_mass_force;
+  ph.scheme_vis = p.scheme_vis;
+  for (int q = 0; q < 3; q++) ph.periodic[q] = p.iperiodic[q] ? 1 : 0;
+  for (int q = 0; q < 6; q++) {
+    ph.bi[q] = p.bound_index[q];
+    ph.sb[q] = p.scheme_boundary[q];
+    ph.ghost[q] = p.ghost_cell[q];
+  }
+  ph.ka1 = p.ka1;
+  ph.kb1 = p.kb1;
+  ph.ka2 = p.ka2;
+  ph.kb2 = p.kb2;
+  ph.ibc = p.ibc;
+  ph.bc_para0 = p.bc_para[0];
+  // OCFD_dxyz_viscous.f90:9-16
+  const double hh[3] = {p.hx, p.hy, p.hz};
+  for (int d = 0; d < 3; d++) {
+    const double h = hh[d];
+    dc.h[d] = h;
+    dc.a1[d] = 1.0 / (60.0 * h);
+    dc.a2[d] = -3.0 / (20.0 * h);
+    dc.a3[d] = 3.0 / (4.0 * h);
+    dc.c1[d] = 0.8 / h;
+    dc.c2[d] = -0.2 / h;
+    dc.c3[d] = 3.80952380952380952e-2 / h;
+    dc.c4[d] = -3.571428571428571428e-3 / h;
+  }
+}
+
+Grid make_grid(const ocfd_params& p) {
+  Grid g;
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.nxh = p.nx + 2 * LAP;
+  g.nyh = p.ny + 2 * LAP;
+  g.nzh = p.nz + 2 * LAP;
+  g.n = (long long)p.nx * p.ny * p.nz;
+  g.nh = (long long)g.nxh * g.nyh * g.nzh;
+  return g;
+}
+
+__global__ void k_fill(double* a, long long n, double v) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a[t] = v;
+}
+__global__ void k_fill32(float* a, long long n, float v) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) a[t] = v;
+}
+// scatter interior (nx,ny,nz) into a haloed array
+__global__ void k_scatter_interior(Grid G, const double* src, double* dst) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nx) + 1, j = (int)((t / G.nx) % G.ny) + 1, k = (int)(t / ((long long)G.nx * G.ny)) + 1;
+    dst[G.ih(i, j, k)] = src[t];
+  }
+}
+// mesh_gen('box') (OCFD_mesh.f90:335-347)
+__global__ void k_box(Grid G, double* X, double* Y, double* Z) {
+  const double PI = 3.1415926535897932;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nx) + 1, j = (int)((t / G.nx) % G.ny) + 1, k = (int)(t / ((long long)G.nx * G.ny)) + 1;
+    const long long h = G.ih(i, j, k);
+    X[h] = 2.0 * PI / (double)G.nx * (double)i;
+    Y[h] = 2.0 * PI / (double)G.ny * (double)j;
+    Z[h] = 2.0 * PI / (double)G.nz * (double)k;
+  }
+}
+
+template <typename R>
+size_t rsize() {
+  return sizeof(R);
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+void ocfd_default_params(ocfd_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->gamma = 1.4;
+  p->re = 100.0;
+  p->ma = 1.0;
+  p->pr = 0.7;
+  p->lap = 4;
+  p->scheme_invis = OCFD_SCHEME_WENO5;
+  p->scheme_vis = OCFD_SCHEME_CD6;
+  p->ref_amu_t0 = 288.15;
+  p->dt = 1.0e-4;
+  p->end_time = 100.0;
+  p->iflag_gridtype = OCFD_GRID3D;
+  p->ibc = OCFD_BC_NONE;
+  p->istep_show = 1;
+  p->istep_save = 1000;
+  p->if_viscous = 1;
+  p->ud7l_diss = 1.0;
+  for (int i = 0; i < 100; i++) p->hybrid_para[i] = 1.0;
+  p->flux_splitting = OCFD_SPLIT_SW;
+}
+
+int ocfd_set_parameters(ocfd_params* p) {
+  if (!p) return OCFD_E_PARAM;
+  if (p->lap != 4) return OCFD_E_PARAM;
+  const int nn[3] = {p->nx, p->ny, p->nz};
+  for (int d = 0; d < 3; d++) {
+    if (nn[d] < 8) return OCFD_E_PARAM;
+    if (!p->iperiodic[d] && nn[d] < 10) return OCFD_E_PARAM;
+  }
+  if (p->scheme_vis != OCFD_SCHEME_CD6 && p->scheme_vis != OCFD_SCHEME_CD8) return OCFD_E_PARAM;
+  if (p->flux_splitting != OCFD_SPLIT_SW && p->flux_splitting != OCFD_SPLIT_LLF) return OCFD_E_PARAM;
+  if (p->ibc != OCFD_BC_NONE && p->ibc != OCFD_BC_BLUNT2D && p->ibc != OCFD_BC_USER_DEF) return OCFD_E_PARAM;
+  if (p->ibc == OCFD_BC_USER_DEF && !(p->bc_para[0] > 0.0)) return OCFD_E_PARAM;
+  for (int q = 0; q < 6; q++) {
+    if (p->scheme_boundary[q] < -1 || p->scheme_boundary[q] > 1) return OCFD_E_PARAM;
+    if (p->ghost_cell[q] < 0 || p->ghost_cell[q] > 2) return OCFD_E_PARAM;
+  }
+  if (p->nfiltering < 0 || p->nfiltering > 10) return OCFD_E_PARAM;
+  if (p->precision != OCFD_PRECISION_FP64 && p->precision != OCFD_PRECISION_MIXED) return OCFD_E_PARAM;
+  // set_parameters: OCFD_readpara.f90:265-270
+  p->hx = 1.0 / (p->nx - 1.0);
+  p->hy = 1.0 / (p->ny - 1.0);
+  p->hz = 1.0 / (p->nz - 1.0);
+  p->cv = 1.0 / (p->gamma * (p->gamma - 1.0) * p->ma * p->ma);
+  p->cp = p->cv * p->gamma;
+  // Bound_index for one rank (:274-283)
+  for (int d = 0; d < 3; d++) {
+    p->bound_index[2 * d] = p->iperiodic[d] == 0 ? 1 : 0;
+    p->bound_index[2 * d + 1] = p->iperiodic[d] == 0 ? 1 : 0;
+  }
+  // stencils (:288-310)
+  switch (p->scheme_invis) {
+    case OCFD_SCHEME_WENO5: p->ka1 = -2; p->kb1 = 2; p->ka2 = -1; p->kb2 = 3; break;
+    case OCFD_SCHEME_WENO7: p->ka1 = -3; p->kb1 = 3; p->ka2 = -2; p->kb2 = 4; break;
+    case OCFD_SCHEME_OMP6:
+    case OCFD_SCHEME_UD7L:
+    case OCFD_SCHEME_HYBRID: p->ka1 = -3; p->kb1 = 4; p->ka2 = -3; p->kb2 = 4; break;
+    default: return OCFD_E_PARAM;
+  }
+  // set_scheme_para (:334-341)
+  const double UD7[8] = {-3.0, 25.0, -101.0, 319.0, 214.0, -38.0, 4.0, 0.0};
+  const double CD8[8] = {-3.0, 29.0, -139.0, 533.0, 533.0, -139.0, 29.0, -3.0};
+  for (int k = 0; k < 8; k++) p->ud7l[k] = p->ud7l_diss * UD7[k] / 420.0 + (1.0 - p->ud7l_diss) * CD8[k] / 840.0;
+  if (p->scheme_invis == OCFD_SCHEME_HYBRID) {
+    const int s = (int)std::llround(p->hybrid_para[0]);
+    if (s != 1 && s != 2) return OCFD_E_PARAM;
+  }
+  return OCFD_OK;
+}
+
+size_t ocfd_gpu_footprint(const ocfd_params* p) {
+  const size_t n = (size_t)p->nx * p->ny * p->nz;
+  const size_t nh = (size_t)(p->nx + 8) * (p->ny + 8) * (p->nz + 8);
+  const bool mixed = p->precision == OCFD_PRECISION_MIXED;
+  const size_t r = mixed ? 4 : 8;
+  const bool chr = p->if_scheme_character != 0;
+  size_t b = 15 * n * 8;                     // f, fn, du
+  b += 6 * nh * 8;                           // prims + second T
+  b += OCFD_N_METRICS * nh * 8 + nh * 8;     // metrics, Rhybrid
+  if (mixed) b += 5 * nh * 4 + OCFD_N_METRICS * nh * 4;
+  const size_t faces = (size_t)(n / p->nx * (p->nx + 1) + n / p->ny * (p->ny + 1) + n / p->nz * (p->nz + 1));
+  b += faces * (chr ? 5 : 10) * r;
+  if (p->if_viscous) b += 12 * n * r;
+  b += 2 * nh * 8 + 4096 * 8;                // scratch
+  return b + (64u << 20);
+}
+
+const char* ocfd_gpu_last_error(const ocfd_handle* h) { return h ? h->err.c_str() : "null handle"; }
+void* ocfd_gpu_stream(ocfd_handle* h) { return h ? (void*)h->st : nullptr; }
+
+int ocfd_gpu_sync(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->st));
+  if (h->hstat->error == 3)
+    return fail(h, OCFD_E_NEGT, "Number of Negative Temperature Points >  Limit, STOP !");
+  return OCFD_OK;
+}
+
+void ocfd_gpu_destroy(ocfd_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (int q = 0; q < 2; q++)
+    if (h->gexec[q]) cudaGraphExecDestroy(h->gexec[q]);
+  auto F = [](void* p) {
+    if (p) cudaFree(p);
+  };
+  F(h->f);
+  F(h->fn);
+  F(h->du);
+  for (int q = 0; q < 5; q++) {
+    F(h->prim[q]);
+    F(h->p32[q]);
+  }
+  F(h->talt);
+  for (int m = 0; m < OCFD_N_METRICS; m++) {
+    F(h->met[m]);
+    F(h->met32[m]);
+  }
+  F(h->rh);
+  for (int q = 0; q < 3; q++) F(h->hf[q]);
+  F(h->ev);
+  F(h->scratch);
+  F(h->dstat);
+  F(h->dout);
+  F(h->dptr);
+  if (h->hstat) cudaFreeHost(h->hstat);
+  if (h->hout) cudaFreeHost(h->hout);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
+  if (!pin || !out) return OCFD_E_PARAM;
+  *out = nullptr;
+  ocfd_params p = *pin;
+  if (ocfd_set_parameters(&p) != OCFD_OK) return OCFD_E_PARAM;
+  ocfd_handle* h = new ocfd_handle();
+  h->p = p;
+  h->device = device;
+  h->g = make_grid(p);
+  fill_phys(p, h->ph, h->dc);
+  h->mixed = p.precision == OCFD_PRECISION_MIXED;
+  h->chr = p.if_scheme_character != 0;
+  bool ghost = false;
+  for (int q = 0; q < 6; q++) ghost = ghost || p.ghost_cell[q] == 1 || p.ghost_cell[q] == 2;
+  h->fuse_bc = p.ibc == OCFD_BC_NONE && !ghost;
+  auto bad = [&](cudaError_t e, const char* w) {
+    std::string m = std::string(w) + ": " + cudaGetErrorString(e);
+    ocfd_gpu_destroy(h);
+    return OCFD_E_CUDA;
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return bad(e, "cudaSetDevice");
+  e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bad(e, "cudaStreamCreate");
+  e = setup_face_kernels();
+  if (e != cudaSuccess) return bad(e, "setup_face_kernels");
+  const Grid& g = h->g;
+  const size_t n = (size_t)g.n, nh = (size_t)g.nh;
+  const size_t r = h->mixed ? 4 : 8;
+#define AL(ptr, bytes)                                       \
+  do {                                                       \
+    e = cudaMalloc((void**)&(ptr), (bytes));                 \
+    if (e != cudaSuccess) { ocfd_gpu_destroy(h); return OCFD_E_NOMEM; } \
+  } while (0)
+  AL(h->f, 5 * n * 8);
+  AL(h->fn, 5 * n * 8);
+  AL(h->du, 5 * n * 8);
+  for (int q = 0; q < 5; q++) AL(h->prim[q], nh * 8);
+  AL(h->talt, nh * 8);
+  for (int m = 0; m < OCFD_N_METRICS; m++) AL(h->met[m], nh * 8);
+  AL(h->rh, nh * 8);
+  if (h->mixed) {
+    for (int q = 0; q < 5; q++) AL(h->p32[q], nh * 4);
+    for (int m = 0; m < OCFD_N_METRICS; m++) AL(h->met32[m], nh * 4);
+  }
+  for (int d = 0; d < 3; d++) {
+    h->fs[d] = g.nfaces(d);
+    AL(h->hf[d], (size_t)h->fs[d] * (h->chr ? 5 : 10) * r);
+  }
+  if (p.if_viscous) AL(h->ev, 12 * n * r);
+  h->scratch_n = std::max(rhybrid_scratch_doubles(g), std::max(2 * nh, reduce_scratch_doubles(g)));
+  AL(h->scratch, h->scratch_n * 8);
+  AL(h->dstat, sizeof(DevStatus));
+  AL(h->dout, 64 * 8);
+  AL(h->dptr, 64 * sizeof(double*));
+#undef AL
+  e = cudaMallocHost((void**)&h->hstat, sizeof(DevStatus));
+  if (e != cudaSuccess) return bad(e, "cudaMallocHost");
+  e = cudaMallocHost((void**)&h->hout, 64 * 8);
+  if (e != cudaSuccess) return bad(e, "cudaMallocHost");
+  memset(h->hstat, 0, sizeof(DevStatus));
+  // allocation values: OCFD_NS_Solver.f90:108-110,139,143-150
+  const int B = 148 * 8;
+  for (int q = 0; q < 5; q++) k_fill<<<B, 256, 0, h->st>>>(h->prim[q], nh, 1.0);
+  k_fill<<<B, 256, 0, h->st>>>(h->talt, nh, 1.0);
+  for (int m = 0; m < OCFD_N_METRICS; m++) k_fill<<<B, 256, 0, h->st>>>(h->met[m], nh, 1.0);
+  k_fill<<<B, 256, 0, h->st>>>(h->rh, nh, 0.0);
+  k_fill<<<B, 256, 0, h->st>>>(h->du, 5 * n, 0.0);
+  k_fill<<<B, 256, 0, h->st>>>(h->f, 5 * n, 0.0);
+  k_fill<<<B, 256, 0, h->st>>>(h->fn, 5 * n, 0.0);
+  if (h->mixed) {
+    for (int q = 0; q < 5; q++) k_fill32<<<B, 256, 0, h->st>>>(h->p32[q], nh, 1.0f);
+    for (int m = 0; m < OCFD_N_METRICS; m++) k_fill32<<<B, 256, 0, h->st>>>(h->met32[m], nh, 1.0f);
+  }
+  e = cudaMemsetAsync(h->dstat, 0, sizeof(DevStatus), h->st);
+  if (e != cudaSuccess) return bad(e, "memset");
+  e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return bad(e, "init");
+  *out = h;
+  return OCFD_OK;
+}
+
+// ------------------------------------------------------------------ mesh / state
+static int refresh_met32(ocfd_handle* h) {
+  if (!h->mixed) return OCFD_OK;
+  for (int m = 0; m < OCFD_N_METRICS; m++) CK(launch_to_f32(h->met[m], h->met32[m], h->g.nh, h->st));
+  return OCFD_OK;
+}
+static int refresh_p32(ocfd_handle* h) {
+  if (!h->mixed) return OCFD_OK;
+  for (int q = 0; q < 5; q++) CK(launch_to_f32(h->prim[q], h->p32[q], h->g.nh, h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_upload_metrics(ocfd_handle* h, const double* const metrics[OCFD_N_METRICS]) {
+  if (!h || !metrics) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  for (int m = 0; m < OCFD_N_METRICS; m++)
+    if (metrics[m]) CK(cudaMemcpyAsync(h->met[m], metrics[m], h->g.nh * 8, cudaMemcpyHostToDevice, h->st));
+  int r = refresh_met32(h);
+  if (r) return r;
+  CK(cudaStreamSynchronize(h->st));
+  h->metrics_ready = true;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const double* z) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  const Grid& g = h->g;
+  if (x && y && z) {
+    double* tmp = h->scratch;  // nh >= n doubles
+    const double* src[3] = {x, y, z};
+    for (int q = 0; q < 3; q++) {
+      CK(cudaMemcpyAsync(tmp, src[q], g.n * 8, cudaMemcpyHostToDevice, h->st));
+      k_scatter_interior<<<148 * 8, 256, 0, h->st>>>(g, tmp, h->met[q]);
+    }
+  } else {
+    k_box<<<148 * 8, 256, 0, h->st>>>(g, h->met[0], h->met[1], h->met[2]);
+  }
+  CK(cudaGetLastError());
+  CK(launch_mesh(g, h->ph, h->dc, h->met, h->p.periodic_span, h->st));
+  int r = refresh_met32(h);
+  if (r) return r;
+  CK(cudaStreamSynchronize(h->st));
+  h->metrics_ready = true;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_download_metrics(ocfd_handle* h, double* const metrics[OCFD_N_METRICS]) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  for (int m = 0; m < OCFD_N_METRICS; m++)
+    if (metrics[m]) CK(cudaMemcpyAsync(metrics[m], h->met[m], h->g.nh * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_upload_state(ocfd_handle* h, const double* f, const double* const prims[5], int istep, double tt) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (f) CK(cudaMemcpyAsync(h->f, f, 5 * h->g.n * 8, cudaMemcpyHostToDevice, h->st));
+  if (prims)
+    for (int q = 0; q < 5; q++)
+      if (prims[q]) CK(cudaMemcpyAsync(h->prim[q], prims[q], h->g.nh * 8, cudaMemcpyHostToDevice, h->st));
+  if (prims && prims[4]) CK(cudaMemcpyAsync(h->talt, h->prim[4], h->g.nh * 8, cudaMemcpyDeviceToDevice, h->st));
+  int r = refresh_p32(h);
+  if (r) return r;
+  CK(cudaStreamSynchronize(h->st));
+  h->istep = istep;
+  h->tt = tt;
+  h->halo_valid = false;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_bc(ocfd_handle* h);
+
+int ocfd_gpu_init3d(ocfd_handle* h, const double* const prims_interior[5], int istep, double tt) {
+  if (!h || !prims_interior) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  const Grid& g = h->g;
+  double* tmp = h->scratch;
+  for (int q = 0; q < 5; q++) {
+    CK(cudaMemcpyAsync(tmp, prims_interior[q], g.n * 8, cudaMemcpyHostToDevice, h->st));
+    k_scatter_interior<<<148 * 8, 256, 0, h->st>>>(g, tmp, h->prim[q]);
+  }
+  CK(launch_init3d(g, h->ph, h->f, h->prim, h->st));
+  CK(cudaMemcpyAsync(h->talt, h->prim[4], g.nh * 8, cudaMemcpyDeviceToDevice, h->st));
+  h->istep = istep;
+  h->tt = tt;
+  h->halo_valid = false;
+  int r = ocfd_gpu_bc(h);
+  if (r) return r;
+  r = refresh_p32(h);
+  if (r) return r;
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_download_state(ocfd_handle* h, double* f, double* const prims[5]) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (f) CK(cudaMemcpyAsync(f, h->f, 5 * h->g.n * 8, cudaMemcpyDeviceToHost, h->st));
+  if (prims)
+    for (int q = 0; q < 5; q++)
+      if (prims[q]) CK(cudaMemcpyAsync(prims[q], h->prim[q], h->g.nh * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+int ocfd_gpu_download_du(ocfd_handle* h, double* du) {
+  if (!h || !du) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(du, h->du, 5 * h->g.n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+int ocfd_gpu_download_rhybrid(ocfd_handle* h, double* rh) {
+  if (!h || !rh) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(rh, h->rh, h->g.nh * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+int ocfd_gpu_get_time(ocfd_handle* h, int* istep, double* tt) {
+  if (!h) return OCFD_E_PARAM;
+  if (istep) *istep = h->istep;
+  if (tt) *tt = h->tt;
+  return OCFD_OK;
+}
+
+// ------------------------------------------------------------------ stage operators
+int ocfd_gpu_save_fn(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->fn, h->f, 5 * h->g.n * 8, cudaMemcpyDeviceToDevice, h->st));
+  return OCFD_OK;
+}
+
+static int halo_all(ocfd_handle* h) {
+  PtrList<double> L;
+  L.n = 5;
+  for (int q = 0; q < 5; q++) L.p[q] = h->prim[q];
+  CK(launch_halo(h->g, h->ph.periodic, L, h->st));
+  if (h->mixed) {
+    PtrList<float> L32;
+    L32.n = 5;
+    for (int q = 0; q < 5; q++) L32.p[q] = h->p32[q];
+    CK(launch_halo_f32(h->g, h->ph.periodic, L32, h->st));
+  }
+  return OCFD_OK;
+}
+
+int ocfd_gpu_halo_prims(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  int r = halo_all(h);
+  if (r) return r;
+  h->halo_valid = true;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_rhybrid(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  if (h->p.scheme_invis != OCFD_SCHEME_HYBRID) return OCFD_OK;
+  CK(cudaSetDevice(h->device));
+  const int sensor = (int)std::llround(h->p.hybrid_para[0]);
+  CK(launch_rhybrid(h->g, h->ph, h->dc, h->prim[0], h->prim[4], h->met, h->rh, h->scratch, sensor,
+                    h->p.hybrid_para, h->st));
+  PtrList<double> L;
+  L.n = 1;
+  L.p[0] = h->rh;
+  CK(launch_halo(h->g, h->ph.periodic, L, h->st));
+  return OCFD_OK;
+}
+
+}  // extern "C"
+
+template <typename R, typename S>
+static int faces(ocfd_handle* h) {
+  const Grid& g = h->g;
+  for (int d = 0; d < 3; d++) {
+    FaceArgs<S> a;
+    a.g = g;
+    a.ph = h->ph;
+    if (std::is_same<S, float>::value) {
+      a.d = (const S*)h->p32[0];
+      a.u = (const S*)h->p32[1];
+      a.v = (const S*)h->p32[2];
+      a.w = (const S*)h->p32[3];
+      a.T = (const S*)h->p32[4];
+      a.A1 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d];
+      a.A2 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 1];
+      a.A3 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 2];
+    } else {
+      a.d = (const S*)h->prim[0];
+      a.u = (const S*)h->prim[1];
+      a.v = (const S*)h->prim[2];
+      a.w = (const S*)h->prim[3];
+      a.T = (const S*)h->prim[4];
+      a.A1 = (const S*)h->met[OCFD_M_AKX1 + 3 * d];
+      a.A2 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 1];
+      a.A3 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 2];
+    }
+    a.rh = h->rh;
+    a.hh = h->hf[d];
+    a.fs = h->fs[d];
+    a.fbeg = h->ph.periodic[d] ? 1 : 0;
+    a.fend = g.len(d);
+    a.split = h->p.flux_splitting;
+    CK((launch_face<R, S>(d, h->chr, h->p.scheme_invis, a, h->st)));
+  }
+  return OCFD_OK;
+}
+
+template <typename R>
+static UpdArgs<R> upd_args(ocfd_handle* h) {
+  UpdArgs<R> a;
+  memset(&a, 0, sizeof(a));
+  a.g = h->g;
+  a.ph = h->ph;
+  a.dc = h->dc;
+  for (int d = 0; d < 3; d++) {
+    a.hf[d] = (const R*)h->hf[d];
+    a.fs[d] = h->fs[d];
+    a.fper[d] = h->ph.periodic[d];
+  }
+  a.h_1[0] = 1.0 / h->p.hx;
+  a.h_1[1] = 1.0 / h->p.hy;
+  a.h_1[2] = 1.0 / h->p.hz;
+  a.ev = (const R*)h->ev;
+  a.ajac = h->met[OCFD_M_AJAC];
+  a.pd = h->prim[0];
+  a.pu = h->prim[1];
+  a.pv = h->prim[2];
+  a.pw = h->prim[3];
+  a.du = h->du;
+  a.f = h->f;
+  a.fn = h->fn;
+  for (int q = 0; q < 4; q++) a.prim[q] = h->prim[q];
+  a.prim[4] = h->talt;  // written; becomes current after the swap
+  a.told = h->prim[4];
+  for (int q = 0; q < 5; q++) a.p32[q] = h->mixed ? h->p32[q] : nullptr;
+  a.st = h->dstat;
+  a.krk = 1;
+  a.fuse_bc = h->fuse_bc ? 1 : 0;
+  a.visc = h->p.if_viscous ? 1 : 0;
+  a.chr = h->chr ? 1 : 0;
+  return a;
+}
+
+extern "C" {
+
+static int inviscous_common(ocfd_handle* h) {
+  CK(cudaSetDevice(h->device));
+  int r = h->mixed ? faces<float, float>(h) : faces<double, double>(h);
+  if (r) return r;
+  if (h->mixed) {
+    CK(launch_div_inv<float>(upd_args<float>(h), h->st));
+  } else {
+    CK(launch_div_inv<double>(upd_args<double>(h), h->st));
+  }
+  return OCFD_OK;
+}
+int ocfd_gpu_du_inviscous(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  if (h->chr) return fail(h, OCFD_E_STATE, "instance is configured for the characteristic form");
+  return inviscous_common(h);
+}
+int ocfd_gpu_du_inviscous_character(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  if (!h->chr) return fail(h, OCFD_E_STATE, "instance is configured for the flux-vector form");
+  return inviscous_common(h);
+}
+
+}  // extern "C"
+
+template <typename R, typename S>
+static int visc_grad(ocfd_handle* h) {
+  ViscArgs<R, S> a;
+  a.g = h->g;
+  a.ph = h->ph;
+  a.dc = h->dc;
+  if (std::is_same<S, float>::value) {
+    a.d = (const S*)h->p32[0];
+    a.u = (const S*)h->p32[1];
+    a.v = (const S*)h->p32[2];
+    a.w = (const S*)h->p32[3];
+    a.T = (const S*)h->p32[4];
+    for (int m = 0; m < 22; m++) a.met[m] = (const S*)h->met32[m];
+  } else {
+    a.d = (const S*)h->prim[0];
+    a.u = (const S*)h->prim[1];
+    a.v = (const S*)h->prim[2];
+    a.w = (const S*)h->prim[3];
+    a.T = (const S*)h->prim[4];
+    for (int m = 0; m < 22; m++) a.met[m] = (const S*)h->met[m];
+  }
+  a.ev = (R*)h->ev;
+  CK((launch_visc_grad<R, S>(a, h->st)));
+  return OCFD_OK;
+}
+
+extern "C" {
+
+int ocfd_gpu_du_viscous(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  if (!h->p.if_viscous) return OCFD_OK;
+  CK(cudaSetDevice(h->device));
+  int r = h->mixed ? visc_grad<float, float>(h) : visc_grad<double, double>(h);
+  if (r) return r;
+  if (h->mixed) {
+    CK(launch_visc_div<float>(upd_args<float>(h), h->st));
+  } else {
+    CK(launch_visc_div<double>(upd_args<double>(h), h->st));
+  }
+  return OCFD_OK;
+}
+
+int ocfd_gpu_rk3(ocfd_handle* h, int krk) {
+  if (!h || krk < 1 || krk > 3) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(launch_rk3(h->g, h->f, h->fn, h->du, h->p.dt, krk, h->st));
+  return OCFD_OK;
+}
+
+static void swap_t(ocfd_handle* h) { std::swap(h->prim[4], h->talt); }
+
+int ocfd_gpu_duvwt(ocfd_handle* h, int* num_negt) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  UpdArgs<double> a = upd_args<double>(h);
+  a.fuse_bc = 0;
+  CK(launch_duvwt(a, h->st));
+  CK(launch_negt_fix(a, h->st));
+  swap_t(h);
+  CK(cudaMemcpyAsync(h->hstat, h->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (num_negt) *num_negt = h->hstat->negt_last;
+  h->halo_valid = false;
+  if (h->hstat->error == 3)
+    return fail(h, OCFD_E_NEGT, "Number of Negative Temperature Points >  Limit, STOP !");
+  return OCFD_OK;
+}
+
+int ocfd_gpu_bc(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
+  CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
+  CK(launch_ghost(h->g, h->ph, h->prim, h->st));
+  return refresh_p32(h);
+}
+
+int ocfd_gpu_filter(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  for (int m = 0; m < h->p.nfiltering; m++) {
+    const double* F = h->p.filter_para[m];
+    const int per = (int)std::llround(F[0]);
+    if (per <= 0 || h->istep % per != 0) continue;
+    CK(launch_filter(h->g, h->ph, h->f, h->scratch, F, h->st));
+  }
+  return OCFD_OK;
+}
+
+int ocfd_gpu_advance_clock(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  h->istep += 1;
+  h->tt += h->p.dt;
+  return OCFD_OK;
+}
+
+// ------------------------------------------------------------------ fused step
+// One RK stage of NS_solver (OCFD_NS_Solver.f90:35-58) on the fused path.
+static int fused_stage(ocfd_handle* h, int krk) {
+  if (krk == 1 && h->p.scheme_invis == OCFD_SCHEME_HYBRID) {
+    int r = ocfd_gpu_rhybrid(h);
+    if (r) return r;
+  }
+  int r = h->mixed ? faces<float, float>(h) : faces<double, double>(h);
+  if (r) return r;
+  if (h->p.if_viscous) {
+    r = h->mixed ? visc_grad<float, float>(h) : visc_grad<double, double>(h);
+    if (r) return r;
+  }
+  if (h->mixed) {
+    UpdArgs<float> a = upd_args<float>(h);
+    a.krk = krk;
+    a.du = nullptr;
+    CK(launch_fused<float>(a, h->st));
+  } else {
+    UpdArgs<double> a = upd_args<double>(h);
+    a.krk = krk;
+    a.du = nullptr;
+    CK(launch_fused<double>(a, h->st));
+  }
+  UpdArgs<double> fx = upd_args<double>(h);
+  CK(launch_negt_fix(fx, h->st));
+  swap_t(h);
+  if (!h->fuse_bc) {
+    CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
+    CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
+    CK(launch_ghost(h->g, h->ph, h->prim, h->st));
+    r = halo_all(h);
+    if (r) return r;
+    r = refresh_p32(h);
+    if (r) return r;
+  }
+  return OCFD_OK;
+}
+
+static int fused_step(ocfd_handle* h) {
+  std::swap(h->f, h->fn);  // fn = f (stage 1 overwrites all of f)
+  for (int krk = 1; krk <= 3; krk++) {
+    int r = fused_stage(h, krk);
+    if (r) return r;
+  }
+  return OCFD_OK;
+}
+
+int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
+  if (!h || nsteps < 0) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (!h->halo_valid) {
+    int r = halo_all(h);
+    if (r) return r;
+    h->halo_valid = true;
+  }
+  const bool use_graph = h->p.nfiltering == 0;
+  for (int s = 0; s < nsteps; s++) {
+    if (!use_graph) {
+      int r = fused_step(h);
+      if (r) return r;
+    } else {
+      const int par = h->parity;
+      if (!h->gexec[par]) {
+        // eager run of this parity once (sets kernel attributes), then capture
+        double* f0 = h->f;
+        double* fn0 = h->fn;
+        double* t0 = h->prim[4];
+        double* ta0 = h->talt;
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int r = fused_step(h);
+        cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+        if (r) return r;
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&h->gexec[par], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+        // capture does not execute: restore the pointers and run the graph
+        h->f = f0;
+        h->fn = fn0;
+        h->prim[4] = t0;
+        h->talt = ta0;
+      }
+      CK(cudaGraphLaunch(h->gexec[par], h->st));
+      std::swap(h->f, h->fn);
+      // three T swaps per step = one net swap
+      std::swap(h->prim[4], h->talt);
+      h->parity ^= 1;
+    }
+    h->istep += 1;
+    h->tt += h->p.dt;
+    if (h->p.nfiltering > 0) {
+      int r = ocfd_gpu_filter(h);
+      if (r) return r;
+    }
+  }
+  if (sync) {
+    CK(cudaMemcpyAsync(h->hstat, h->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st));
+    return ocfd_gpu_sync(h);
+  }
+  return OCFD_OK;
+}
+
+// ------------------------------------------------------------------ diagnostics
+int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]) {
+  if (!h || !E0) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(launch_flow_msg(h->g, h->ph, h->f, h->prim, h->met[OCFD_M_AJAC], h->scratch, h->dout, h->st));
+  CK(cudaMemcpyAsync(h->hout, h->dout, 3 * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  const double N = (double)(h->p.nx * h->p.ny * h->p.nz);
+  for (int q = 0; q < 3; q++) E0[q] = h->hout[q] / N;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_ana_box(ocfd_handle* h, double out[20]) {
+  if (!h || !out) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  int r = halo_all(h);  // the reference exchanges u, v, w first (OCFD_ANA.f90:194-207)
+  if (r) return r;
+  CK(launch_ana_box(h->g, h->ph, h->dc, h->prim, h->met, h->scratch, h->dout, h->dout + 16, h->st));
+  CK(cudaMemcpyAsync(h->hout, h->dout, 17 * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  const double N = (double)(h->p.nx * h->p.ny * h->p.nz);
+  double a[14];
+  for (int q = 0; q < 14; q++) a[q] = h->hout[q] / N;
+  double u_rms = a[0], v_rms = a[1], w_rms = a[2], Ux_rms = a[3], Ux_sk = a[4], Ux_fl = a[5], d_aver = a[6];
+  double c_aver = a[7], Amu_aver = a[8], E_k = a[9], T_aver = a[10], u_sk = a[11], u_fl = a[12];
+  double ens = 0.5 * a[13];
+  // OCFD_ANA.f90:258-287
+  const double VV_rms = std::sqrt((u_rms + v_rms + w_rms) / 3.0);
+  const double Amt = std::sqrt(u_rms + v_rms + w_rms) / c_aver;
+  u_rms = std::sqrt(u_rms);
+  v_rms = std::sqrt(v_rms);
+  w_rms = std::sqrt(w_rms);
+  Ux_rms = std::sqrt(Ux_rms);
+  const double Alamda = VV_rms / Ux_rms, Alamdax = u_rms / Ux_rms;
+  const double Re_lamda = VV_rms * Alamda * d_aver / Amu_aver;
+  const double Re_lamdax = VV_rms * Alamdax * d_aver / Amu_aver;
+  Ux_sk = Ux_sk / (Ux_rms * Ux_rms * Ux_rms);
+  Ux_fl = Ux_fl / ((Ux_rms * Ux_rms) * (Ux_rms * Ux_rms));
+  u_sk = u_sk / (u_rms * u_rms * u_rms);
+  u_fl = u_fl / ((u_rms * u_rms) * (u_rms * u_rms));
+  const double d_rms = std::sqrt(h->hout[16] / N);
+  const double res[20] = {h->tt, Re_lamda, Re_lamdax, Amt, VV_rms, u_rms, v_rms, w_rms, u_sk, u_fl,
+                          Ux_sk, Ux_fl, E_k, ens, d_rms, T_aver, Amu_aver, d_aver, Ux_rms, Alamdax};
+  memcpy(out, res, sizeof(res));
+  return OCFD_OK;
+}
+
+// ------------------------------------------------------------------ batch (ensemble)
+struct ocfd_batch {
+  std::vector<ocfd_handle*> m;
+  cudaStream_t st = nullptr;
+  std::vector<cudaEvent_t> ev;
+};
+
+int ocfd_batch_create(ocfd_handle* const* members, int count, ocfd_batch** out) {
+  if (!members || count <= 0 || !out) return OCFD_E_PARAM;
+  ocfd_batch* b = new ocfd_batch();
+  for (int q = 0; q < count; q++) b->m.push_back(members[q]);
+  *out = b;
+  return OCFD_OK;
+}
+
+int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
+  if (!b) return OCFD_E_PARAM;
+  // the members' streams run concurrently; each advances from its own graph
+  for (ocfd_handle* h : b->m) {
+    int r = ocfd_gpu_step(h, nsteps, 0);
+    if (r) return r;
+  }
+  if (sync)
+    for (ocfd_handle* h : b->m) {
+      int r = ocfd_gpu_step(h, 0, 1);
+      if (r) return r;
+    }
+  return OCFD_OK;
+}
+
+void ocfd_batch_destroy(ocfd_batch* b) { delete b; }
+
+}  // extern "C"

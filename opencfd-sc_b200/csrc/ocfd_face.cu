@@ -1,0 +1,526 @@
+// ocfd_face.cu -- face-flux kernels of the inviscous terms, one launch per
+// direction: split -> (characteristic projection) -> reconstruction, written
+// as numerical fluxes h(i+1/2) per face.  The flux difference, the Jacobian
+// scaling and the rest of the stage happen in the update kernel
+// (ocfd_update.cu), which reads these faces.
+//
+// Reference: du_inviscous (OCFD_inviscous.f90:53-203) with OCFD2d_flux1/2
+// (:210-361) for the flux-vector form, du_inviscous_Character
+// (OCFD_inviscous_character.f90:3-159) with flux_charteric / flux_x1 / flux_x2
+// (:162-416) for the characteristic form.
+//
+// Tiling: a block owns NP pencils x TF consecutive faces along the sweep
+// direction (NP*TF = 256 threads, one face per thread).  Phase 1 loads the
+// TF+7 points of its stencil (coalesced along i for x, across i for y/z),
+// computes the split fluxes once per point and stages them in shared memory.
+// Phase 2 computes one face per thread from a register window of 8 points.
+// For a periodic direction face 0 equals face n bit for bit, so only faces
+// 1..n are computed: n faces for n points, no tile does extra work.
+#include <cstring>
+
+#include "ocfd_device.cuh"
+#include "ocfd_kernels.h"
+#include "ocfd_schemes.cuh"
+
+namespace ocfd {
+
+template <int DIR>
+struct FaceTile;
+template <>
+struct FaceTile<0> {
+  static constexpr int NP = 4, TF = 64;
+};
+template <>
+struct FaceTile<1> {
+  static constexpr int NP = 16, TF = 16;
+};
+template <>
+struct FaceTile<2> {
+  static constexpr int NP = 16, TF = 16;
+};
+
+// ---------------------------------------------------------------------------
+// Flux-vector form, boundary-aware reconstruction of one face (OCFD2d_flux1).
+template <int SCHEME, typename R>
+__device__ __forceinline__ R nc_flux1_bnd(const R* v, const R* U, int g, int nn, int ihy, const Phys& ph, int dir) {
+  const int bi0 = ph.bi[2 * dir], bi1 = ph.bi[2 * dir + 1], sb0 = ph.sb[2 * dir], sb1 = ph.sb[2 * dir + 1];
+  const int Ka = ph.ka1, Kb = ph.kb1;
+  const int ib = (bi0 == 0 || sb0 == -1) ? 0 : -Ka + 1;
+  const int ie = (bi1 == 0 || sb1 == -1) ? nn : nn - Kb;
+  R h = R(0);
+  if (g >= ib && g <= ie) h = schemeP<SCHEME>(v, U, ihy);
+  if (bi0 == 1 && g <= -Ka) {
+    if (sb0 == 0) {
+      if (g == 0)
+        h = (R(2) * v[1] + R(5) * v[2] - v[3]) / R(6);
+      else if (g == 1)
+        h = (R(2) * v[0] + R(5) * v[1] - v[2]) / R(6);
+      else if (g == 2)
+        h = weno5P_bnd(v, 1);
+      else
+        h = weno5P(v);
+    } else if (sb0 == 1) {
+      h = weno5P(v);
+    }
+  }
+  if (bi1 == 1 && g >= nn - Kb + 1) {
+    if (sb1 == 0) {
+      if (g == nn)
+        h = (R(2) * v[-2] - R(7) * v[-1] + R(11) * v[0]) / R(6);
+      else if (g == nn - 1)
+        h = weno5P_bnd(v, 2);
+      else
+        h = weno5P(v);
+    } else if (sb1 == 1) {
+      h = weno5P(v);
+    }
+  }
+  return h;
+}
+
+// OCFD2d_flux2 (OCFD_inviscous.f90:287-361)
+template <int SCHEME, typename R>
+__device__ __forceinline__ R nc_flux2_bnd(const R* v, const R* U, int g, int nn, int ihy, const Phys& ph, int dir) {
+  const int bi0 = ph.bi[2 * dir], bi1 = ph.bi[2 * dir + 1], sb0 = ph.sb[2 * dir], sb1 = ph.sb[2 * dir + 1];
+  const int Ka = ph.ka2, Kb = ph.kb2;
+  const int ib = (bi0 == 0 || sb0 == -1) ? 0 : -Ka + 1;
+  const int ie = (bi1 == 0 || sb1 == -1) ? nn : nn - Kb;
+  R h = R(0);
+  if (g >= ib && g <= ie) h = schemeM<SCHEME>(v, U, ihy);
+  if (bi0 == 1 && g <= -Ka) {
+    if (sb0 == 0) {
+      if (g == 0)
+        h = (R(2) * v[3] - R(7) * v[2] + R(11) * v[1]) / R(6);
+      else if (g == 1)
+        h = weno5M_bnd(v, 1);
+      else
+        h = weno5M(v);
+    } else if (sb0 == 1) {
+      h = weno5M(v);
+    }
+  }
+  if (bi1 == 1 && g >= nn - Kb + 1) {
+    if (sb1 == 0) {
+      if (g == nn)
+        h = (R(2) * v[0] + R(5) * v[-1] - v[-2]) / R(6);
+      else if (g == nn - 1)
+        h = (R(2) * v[1] + R(5) * v[0] - v[-1]) / R(6);
+      else if (g == nn - 2)
+        h = weno5M_bnd(v, 2);
+      else
+        h = weno5M(v);
+    } else if (sb1 == 1) {
+      h = weno5M(v);
+    }
+  }
+  return h;
+}
+
+// Characteristic form: flux_x1 (OCFD_inviscous_character.f90:313-364) for a
+// face that is not an interior face.
+template <typename R>
+__device__ __forceinline__ R ch_flux1_bnd(const R* ff, int g, int nn, const Phys& ph, int dir) {
+  const int bi0 = ph.bi[2 * dir], bi1 = ph.bi[2 * dir + 1], sb0 = ph.sb[2 * dir], sb1 = ph.sb[2 * dir + 1];
+  const int Ka = ph.ka1, Kb = ph.kb1;
+  if (g <= -Ka && bi0 == 1 && sb0 != -1) {
+    if (sb0 == 0) {
+      if (g == 1) return (R(2) * ff[0] + R(5) * ff[1] - ff[2]) / R(6);
+      if (g == 2) return weno5P_bnd(ff, 1);
+      return weno5P(ff);
+    } else if (sb0 == 1) {
+      return weno5P(ff);
+    }
+  } else if (g > nn - Kb && bi1 == 1 && sb1 != -1) {
+    if (sb1 == 0) {
+      if (g == nn - 1) return weno5P_bnd(ff, 2);
+      return weno5P(ff);
+    } else if (sb1 == 1) {
+      return weno5P(ff);
+    }
+  }
+  return R(0);
+}
+
+// flux_x2 (OCFD_inviscous_character.f90:367-416), non-interior face
+template <typename R>
+__device__ __forceinline__ R ch_flux2_bnd(const R* ff, int g, int nn, const Phys& ph, int dir) {
+  const int bi0 = ph.bi[2 * dir], bi1 = ph.bi[2 * dir + 1], sb0 = ph.sb[2 * dir], sb1 = ph.sb[2 * dir + 1];
+  const int Ka = ph.ka2, Kb = ph.kb2;
+  if (g <= -Ka && bi0 == 1 && sb0 != -1) {
+    if (sb0 == 0) {
+      if (g == 1) return weno5M_bnd(ff, 1);
+      return weno5M(ff);
+    } else if (sb0 == 1) {
+      return weno5M(ff);
+    }
+  } else if (g > nn - Kb && bi1 == 1 && sb1 != -1) {
+    if (sb1 == 0) {
+      if (g == nn - 1) return (R(2) * ff[1] + R(5) * ff[0] - ff[-1]) / R(6);
+      if (g == nn - 2) return weno5M_bnd(ff, 2);
+      return weno5M(ff);
+    } else if (sb1 == 1) {
+      return weno5M(ff);
+    }
+  }
+  return R(0);
+}
+
+// Stencil ranges of the projected values each scheme reads (set_parameters,
+// OCFD_readpara.f90:288-315).  The hybrid's WENO5/WENO7 faces read subsets.
+template <int SCHEME>
+struct Stencil {
+  static constexpr int PLO = -3, PHI = 4, MLO = -3, MHI = 4;
+};
+template <>
+struct Stencil<SCH_WENO7> {
+  static constexpr int PLO = -3, PHI = 3, MLO = -2, MHI = 4;
+};
+template <>
+struct Stencil<SCH_WENO5> {
+  static constexpr int PLO = -2, PHI = 2, MLO = -1, MHI = 3;
+};
+
+// ---------------------------------------------------------------------------
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+__global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
+  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
+  // shared memory: 10 split-flux arrays (+7 face-state arrays for CHAR)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  auto SI = [](int var, int l, int p) -> int { return var * (NP * LT) + (DIR == 0 ? p * LT + l : l * NP + p); };
+
+  const Grid& G = a.g;
+  const Phys& ph = a.ph;
+  const int nn = G.len(DIR);
+  int g0, pbase;
+  if (DIR == 0) {
+    g0 = a.fbeg + blockIdx.x * TF;
+    pbase = blockIdx.y * NP;
+  } else {
+    g0 = a.fbeg + blockIdx.y * TF;
+    pbase = blockIdx.x * NP;
+  }
+  // pencil p -> (i,j,k) with the along-direction index left at 0
+  auto pencil = [&](int p, int& i, int& j, int& k) -> bool {
+    if (DIR == 0) {
+      int pen = pbase + p;
+      i = 0;
+      j = pen % G.ny + 1;
+      k = pen / G.ny + 1;
+      return pen < G.ny * G.nz;
+    } else if (DIR == 1) {
+      i = pbase + p + 1;
+      j = 0;
+      k = blockIdx.z + 1;
+      return i <= G.nx;
+    } else {
+      i = pbase + p + 1;
+      j = blockIdx.z + 1;
+      k = 0;
+      return i <= G.nx;
+    }
+  };
+  const long long hs = G.hstride(DIR);
+  const R gam = R(ph.gamma), ma = R(ph.ma);
+
+  // ---- phase 1: split fluxes of the tile's points into shared memory
+  for (int t = threadIdx.x; t < NP * LT; t += blockDim.x) {
+    int l, p;
+    if (DIR == 0) {
+      l = t % LT;
+      p = t / LT;
+    } else {
+      p = t % NP;
+      l = t / NP;
+    }
+    int i, j, k;
+    bool ok = pencil(p, i, j, k);
+    const int gl = g0 - 3 + l;  // point index along DIR
+    ok = ok && gl <= nn + LAP;
+    R d = R(1), u = R(1), v = R(1), w = R(1), T = R(1), A1 = R(1), A2 = R(1), A3 = R(1);
+    if (ok) {
+      long long h = G.ih(i, j, k) + (long long)gl * hs;
+      d = R(__ldg(a.d + h));
+      u = R(__ldg(a.u + h));
+      v = R(__ldg(a.v + h));
+      w = R(__ldg(a.w + h));
+      T = R(__ldg(a.T + h));
+      A1 = R(__ldg(a.A1 + h));
+      A2 = R(__ldg(a.A2 + h));
+      A3 = R(__ldg(a.A3 + h));
+    }
+    const R c = sqrt(T) / ma;  // cc: OCFD_inviscous.f90:67
+    R fp[5], fm[5];
+    if (a.split == 1)
+      split_sw(gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+    else
+      split_llf(gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      sm[SI(m, l, p)] = fp[m];
+      sm[SI(5 + m, l, p)] = fm[m];
+    }
+    if (CHAR) {
+      sm[SI(10, l, p)] = u;
+      sm[SI(11, l, p)] = v;
+      sm[SI(12, l, p)] = w;
+      sm[SI(13, l, p)] = c;
+      sm[SI(14, l, p)] = A1;
+      sm[SI(15, l, p)] = A2;
+      sm[SI(16, l, p)] = A3;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: one face per thread
+  R U[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) U[q] = R(ph.ud7l[q]);
+  R* out = reinterpret_cast<R*>(a.hh);
+
+  for (int t = threadIdx.x; t < NP * TF; t += blockDim.x) {
+    int f, p;
+    if (DIR == 0) {
+      f = t % TF;
+      p = t / TF;
+    } else {
+      p = t % NP;
+      f = t / NP;
+    }
+    int i, j, k;
+    if (!pencil(p, i, j, k)) continue;
+    const int g = g0 + f;
+    if (g > a.fend) continue;
+    int ii = DIR == 0 ? g : i, jj = DIR == 1 ? g : j, kk = DIR == 2 ? g : k;
+    const long long fo = G.face(DIR, g, ii, jj, kk);
+    int ihy = 0;
+    if (SCHEME == SCH_HYBRID) {
+      // OCFD_inviscous.f90:76-81: Rhb0 = max(Rhybrid(g), Rhybrid(g+1))
+      long long h = G.ih(i, j, k) + (long long)g * hs;
+      double r0 = __ldg(a.rh + h), r1 = __ldg(a.rh + h + hs);
+      ihy = hybrid_index(rmax(r0, r1), ph.hyb1, ph.hyb2);
+    }
+    const int bi0 = ph.bi[2 * DIR], bi1 = ph.bi[2 * DIR + 1], sb0 = ph.sb[2 * DIR], sb1 = ph.sb[2 * DIR + 1];
+
+    if (!CHAR) {
+      // ---- flux-vector form: h1 (F+) and h2 (F-) per variable
+      const int ib1 = (bi0 == 0 || sb0 == -1) ? 0 : -ph.ka1 + 1, ie1 = (bi1 == 0 || sb1 == -1) ? nn : nn - ph.kb1;
+      const int ib2 = (bi0 == 0 || sb0 == -1) ? 0 : -ph.ka2 + 1, ie2 = (bi1 == 0 || sb1 == -1) ? nn : nn - ph.kb2;
+      const bool inner = g >= ib1 && g <= ie1 && g >= ib2 && g <= ie2;
+#pragma unroll 1
+      for (int m = 0; m < 5; m++) {
+        R wv[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) wv[q] = sm[SI(m, f + q, p)];
+        R h1 = inner ? schemeP<SCHEME>(wv + 3, U, ihy) : nc_flux1_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
+#pragma unroll
+        for (int q = 0; q < 8; q++) wv[q] = sm[SI(5 + m, f + q, p)];
+        R h2 = inner ? schemeM<SCHEME>(wv + 3, U, ihy) : nc_flux2_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
+        out[fo + (long long)m * a.fs] = h1;
+        out[fo + (long long)(5 + m) * a.fs] = h2;
+      }
+    } else {
+      // ---- characteristic form (flux_charteric)
+      const int ia = (bi0 == 0 || sb0 != 0) ? 0 : 1;
+      const int ibf = (bi1 == 0 || sb1 != 0) ? nn : nn - 1;
+      R hh[5];
+      if (g < ia || g > ibf) {
+        // non-reflecting boundary faces, OCFD_inviscous_character.f90:295-309
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+          R fpv[8], fmv[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            fpv[q] = sm[SI(m, f + q, p)];
+            fmv[q] = sm[SI(5 + m, f + q, p)];
+          }
+          const R* P = fpv + 3;
+          const R* M = fmv + 3;
+          if (g == 0)
+            hh[m] = (R(2) * P[1] + R(5) * P[2] - P[3] + R(2) * M[3] - R(7) * M[2] + R(11) * M[1]) / R(6);
+          else
+            hh[m] = (R(2) * P[-2] - R(7) * P[-1] + R(11) * P[0] + R(2) * M[0] + R(5) * M[-1] - M[-2]) / R(6);
+        }
+      } else {
+        const bool inner1 = (bi0 == 0 || g > -ph.ka1 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb1 || sb1 == -1);
+        const bool inner2 = (bi0 == 0 || g > -ph.ka2 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb2 || sb1 == -1);
+        if (ihy == 1) {
+          // linear hybrid face: no characteristic projection (:192-194, :281-282)
+#pragma unroll 1
+          for (int m = 0; m < 5; m++) {
+            R wv[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) wv[q] = sm[SI(m, f + q, p)];
+            R h1 = inner1 ? schemeP<SCHEME>(wv + 3, U, ihy) : ch_flux1_bnd(wv + 3, g, nn, ph, DIR);
+#pragma unroll
+            for (int q = 0; q < 8; q++) wv[q] = sm[SI(5 + m, f + q, p)];
+            R h2 = inner2 ? schemeM<SCHEME>(wv + 3, U, ihy) : ch_flux2_bnd(wv + 3, g, nn, ph, DIR);
+            hh[m] = h1 + h2;
+          }
+        } else {
+          // face state: arithmetic means of the two neighbours (:205-211)
+          const int sL = f + 3, sR = f + 4;
+          const R u1 = (sm[SI(10, sL, p)] + sm[SI(10, sR, p)]) * R(0.5);
+          const R v1 = (sm[SI(11, sL, p)] + sm[SI(11, sR, p)]) * R(0.5);
+          const R w1 = (sm[SI(12, sL, p)] + sm[SI(12, sR, p)]) * R(0.5);
+          const R c1 = (sm[SI(13, sL, p)] + sm[SI(13, sR, p)]) * R(0.5);
+          const R a1 = (sm[SI(14, sL, p)] + sm[SI(14, sR, p)]) * R(0.5);
+          const R a2 = (sm[SI(15, sL, p)] + sm[SI(15, sR, p)]) * R(0.5);
+          const R a3 = (sm[SI(16, sL, p)] + sm[SI(16, sR, p)]) * R(0.5);
+          // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
+          R ss = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+          const R n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
+          R l1, l2, l3;
+          if (fabs(n3) <= fabs(n2)) {
+            ss = sqrt(n1 * n1 + n2 * n2);
+            l1 = -n2 / ss;
+            l2 = n1 / ss;
+            l3 = R(0);
+          } else {
+            ss = sqrt(n1 * n1 + n3 * n3);
+            l1 = -n3 / ss;
+            l2 = R(0);
+            l3 = n1 / ss;
+          }
+          const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+          const R un = u1 * n1 + v1 * n2 + w1 * n3;
+          const R ul = u1 * l1 + v1 * l2 + w1 * l3;
+          const R um = u1 * m1 + v1 * m2 + w1 * m3;
+          const R V2 = (u1 * u1 + v1 * v1 + w1 * w1) * R(0.5);
+          const R KK = (R(ph.gamma) - R(1)) / (c1 * c1);
+          const R KK1 = KK * R(0.5);
+          const R X1 = R(1) / (R(2) * c1);
+          const R L[5][5] = {{R(1) - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
+                             {-ul, l1, l2, l3, R(0)},
+                             {-um, m1, m2, m3, R(0)},
+                             {KK1 * V2 + X1 * un, -X1 * n1 - KK1 * u1, -X1 * n2 - KK1 * v1, -X1 * n3 - KK1 * w1, KK1},
+                             {KK1 * V2 - X1 * un, X1 * n1 - KK1 * u1, X1 * n2 - KK1 * v1, X1 * n3 - KK1 * w1, KK1}};
+          R h0[5];
+          // ---- F+ projected onto the characteristic variables (:254-261), reconstructed
+          {
+            R q[5][8];
+            constexpr int LO = Stencil<SCHEME>::PLO, HI = Stencil<SCHEME>::PHI;
+#pragma unroll
+            for (int s = LO; s <= HI; s++) {
+              const int l = f + 3 + s;
+              const R f0 = sm[SI(0, l, p)], f1 = sm[SI(1, l, p)], f2 = sm[SI(2, l, p)], f3 = sm[SI(3, l, p)],
+                      f4 = sm[SI(4, l, p)];
+              q[0][s + 3] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
+              q[1][s + 3] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
+              q[2][s + 3] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
+              q[3][s + 3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
+              q[4][s + 3] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
+            }
+#pragma unroll
+            for (int s = -3; s <= 4; s++)
+              if (s < LO || s > HI)
+#pragma unroll
+                for (int r = 0; r < 5; r++) q[r][s + 3] = R(0);
+#pragma unroll
+            for (int r = 0; r < 5; r++)
+              h0[r] = inner1 ? schemeP<SCHEME>(q[r] + 3, U, ihy) : ch_flux1_bnd(q[r] + 3, g, nn, ph, DIR);
+          }
+          // ---- F- (:264-271)
+          {
+            R q[5][8];
+            constexpr int LO = Stencil<SCHEME>::MLO, HI = Stencil<SCHEME>::MHI;
+#pragma unroll
+            for (int s = LO; s <= HI; s++) {
+              const int l = f + 3 + s;
+              const R f0 = sm[SI(5, l, p)], f1 = sm[SI(6, l, p)], f2 = sm[SI(7, l, p)], f3 = sm[SI(8, l, p)],
+                      f4 = sm[SI(9, l, p)];
+              q[0][s + 3] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
+              q[1][s + 3] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
+              q[2][s + 3] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
+              q[3][s + 3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
+              q[4][s + 3] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
+            }
+#pragma unroll
+            for (int s = -3; s <= 4; s++)
+              if (s < LO || s > HI)
+#pragma unroll
+                for (int r = 0; r < 5; r++) q[r][s + 3] = R(0);
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              R h2 = inner2 ? schemeM<SCHEME>(q[r] + 3, U, ihy) : ch_flux2_bnd(q[r] + 3, g, nn, ph, DIR);
+              h0[r] = h0[r] + h2;
+            }
+          }
+          // ---- back to physical space, hh = R h0 (:284-288); R = S^-1 (:244-248)
+          const R H = V2 + R(1) / KK;
+          hh[0] = h0[0] + h0[3] + h0[4];
+          hh[1] = u1 * h0[0] + l1 * h0[1] + m1 * h0[2] + (u1 - c1 * n1) * h0[3] + (u1 + c1 * n1) * h0[4];
+          hh[2] = v1 * h0[0] + l2 * h0[1] + m2 * h0[2] + (v1 - c1 * n2) * h0[3] + (v1 + c1 * n2) * h0[4];
+          hh[3] = w1 * h0[0] + l3 * h0[1] + m3 * h0[2] + (w1 - c1 * n3) * h0[3] + (w1 + c1 * n3) * h0[4];
+          hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - c1 * un) * h0[3] + (H + c1 * un) * h0[4];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; m++) out[fo + (long long)m * a.fs] = hh[m];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
+  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
+  constexpr int NV = CHAR ? 17 : 10;  // split fluxes (+ face state)
+  const size_t smem = (size_t)NV * NP * LT * sizeof(R);
+  auto kern = k_face<DIR, CHAR, SCHEME, R, S>;
+  if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int nf = a.fend - a.fbeg + 1;
+  dim3 grid;
+  if (DIR == 0) {
+    grid = dim3((nf + TF - 1) / TF, (a.g.ny * a.g.nz + NP - 1) / NP, 1);
+  } else {
+    grid = dim3((a.g.nx + NP - 1) / NP, (nf + TF - 1) / TF, DIR == 1 ? a.g.nz : a.g.ny);
+  }
+  kern<<<grid, NP * TF, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, typename S>
+cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st) {
+#define OCFD_FACE_CASE(D, C, SC) \
+  if (dir == D && chr == C && scheme == SC) return launch_face_t<D, C, SC, R, S>(a, st);
+#define OCFD_FACE_SCHEMES(D, C)         \
+  OCFD_FACE_CASE(D, C, SCH_WENO5)       \
+  OCFD_FACE_CASE(D, C, SCH_WENO7)       \
+  OCFD_FACE_CASE(D, C, SCH_OMP6)        \
+  OCFD_FACE_CASE(D, C, SCH_UD7L)        \
+  OCFD_FACE_CASE(D, C, SCH_HYBRID)
+  OCFD_FACE_SCHEMES(0, false)
+  OCFD_FACE_SCHEMES(1, false)
+  OCFD_FACE_SCHEMES(2, false)
+  OCFD_FACE_SCHEMES(0, true)
+  OCFD_FACE_SCHEMES(1, true)
+  OCFD_FACE_SCHEMES(2, true)
+#undef OCFD_FACE_SCHEMES
+#undef OCFD_FACE_CASE
+  return cudaErrorInvalidValue;
+}
+
+template cudaError_t launch_face<double, double>(int, bool, int, const FaceArgs<double>&, cudaStream_t);
+template cudaError_t launch_face<float, float>(int, bool, int, const FaceArgs<float>&, cudaStream_t);
+
+// A FaceArgs with an empty grid asks launch_face_t to set the kernel's
+// shared-memory attribute instead of launching it.
+cudaError_t setup_face_kernels() {
+  const int schemes[5] = {SCH_WENO5, SCH_WENO7, SCH_OMP6, SCH_UD7L, SCH_HYBRID};
+  FaceArgs<double> ad;
+  FaceArgs<float> af;
+  memset(&ad, 0, sizeof(ad));
+  memset(&af, 0, sizeof(af));
+  for (int d = 0; d < 3; d++)
+    for (int c = 0; c < 2; c++)
+      for (int s = 0; s < 5; s++) {
+        cudaError_t e = launch_face<double, double>(d, c == 1, schemes[s], ad, 0);
+        if (e != cudaSuccess) return e;
+        e = launch_face<float, float>(d, c == 1, schemes[s], af, 0);
+        if (e != cudaSuccess) return e;
+      }
+  return cudaSuccess;
+}
+
+}  // namespace ocfd

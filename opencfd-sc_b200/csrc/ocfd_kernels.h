@@ -1,0 +1,131 @@
+// ocfd_kernels.h -- launch interface between the instance code (ocfd_api.cu)
+// and the kernels (ocfd_face.cu, ocfd_update.cu, ocfd_aux.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ocfd_device.cuh"
+
+namespace ocfd {
+
+// Central-difference coefficients per direction (OCFD_dxyz_viscous.f90:9-16).
+struct DCoef {
+  double h[3];
+  double a1[3], a2[3], a3[3];          // CD6
+  double c1[3], c2[3], c3[3], c4[3];   // CD8
+};
+
+// Arguments of the viscous-gradient kernel (stress and heat flux -> Ev).
+template <typename R, typename S>
+struct ViscArgs {
+  Grid g;
+  Phys ph;
+  DCoef dc;
+  const S* d;
+  const S* u;
+  const S* v;
+  const S* w;
+  const S* T;
+  const S* met[22];  // haloed metrics (OCFD_M_* order); S = double or float copies
+  R* ev;             // 12 interior arrays: Ev1(1..4), Ev2(1..4), Ev3(1..4)
+};
+
+// Arguments of the stage-tail kernels (flux difference, viscous divergence,
+// RK3, primitive recovery, face refresh, periodic halo).
+template <typename R>
+struct UpdArgs {
+  Grid g;
+  Phys ph;
+  DCoef dc;
+  const R* hf[3];      // face fluxes of x, y, z
+  long long fs[3];     // per-variable strides
+  int fper[3];         // faces stored 1..n (periodic: face 0 == face n)
+  double h_1[3];       // 1/hx, 1/hy, 1/hz
+  const R* ev;         // viscous fluxes (12 interior arrays) or nullptr
+  const double* ajac;  // haloed Ajac
+  const double* pd;    // haloed d,u,v,w (mass force)
+  const double* pu;
+  const double* pv;
+  const double* pw;
+  double* du;          // 5 interior arrays
+  double* f;
+  const double* fn;
+  double* prim[5];     // haloed d,u,v,w,T (T: the buffer being written)
+  const double* told;  // haloed T of the previous stage (negative-T repair)
+  float* p32[5];       // FP32 copies of the primitives (mixed precision) or nullptr
+  DevStatus* st;
+  int krk;
+  int fuse_bc;         // BC_None without ghost cells: face refresh + halo in-kernel
+  int visc;
+  int chr;
+};
+
+// A short list of device arrays passed by value (safe inside captured graphs).
+template <typename T>
+struct PtrList {
+  T* p[16];
+  int n;
+};
+
+template <typename R, typename S>
+cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st);
+// raise the dynamic shared-memory limit of every face kernel (call outside graph capture)
+cudaError_t setup_face_kernels();
+
+template <typename R, typename S>
+cudaError_t launch_visc_grad(const ViscArgs<R, S>& a, cudaStream_t st);
+
+// du = inviscous flux divergence (+ mass force)
+template <typename R>
+cudaError_t launch_div_inv(const UpdArgs<R>& a, cudaStream_t st);
+// du(2:5) += viscous divergence
+template <typename R>
+cudaError_t launch_visc_div(const UpdArgs<R>& a, cudaStream_t st);
+// the whole stage tail in one pass
+template <typename R>
+cudaError_t launch_fused(const UpdArgs<R>& a, cudaStream_t st);
+
+cudaError_t launch_rk3(const Grid& g, double* f, const double* fn, const double* du, double dt, int krk,
+                       cudaStream_t st);
+// primitive recovery (+ negative-T detection, FP32 copies)
+cudaError_t launch_duvwt(const UpdArgs<double>& a, cudaStream_t st);
+// serial in-order repair of the points with T <= 0 (handle_NegativeT)
+cudaError_t launch_negt_fix(const UpdArgs<double>& a, cudaStream_t st);
+
+// periodic face halo of narr haloed arrays (exchange_boundary_xyz)
+cudaError_t launch_halo(const Grid& g, const int periodic[3], PtrList<double> arrs, cudaStream_t st);
+cudaError_t launch_halo_f32(const Grid& g, const int periodic[3], PtrList<float> arrs, cudaStream_t st);
+// BC dispatch on the primitives (blunt2d / user isothermal wall)
+cudaError_t launch_bc_wall(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
+// f refresh on the six faces from the primitives (OCFD_BC.f90:150-218)
+cudaError_t launch_bc_refresh(const Grid& g, const Phys& ph, double* f, double* const prim[5], cudaStream_t st);
+// Flow_Ghost_Extent_2nd
+cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
+// FP32 copies of the primitives
+cudaError_t launch_to_f32(const double* src, float* dst, long long n, cudaStream_t st);
+// init3d: f from primitives
+cudaError_t launch_init3d(const Grid& g, const Phys& ph, double* f, double* const prim[5], cudaStream_t st);
+
+// comput_Rhybrid; scratch holds p (haloed) and reduction partials
+cudaError_t launch_rhybrid(const Grid& g, const Phys& ph, const DCoef& dc, const double* d, const double* T,
+                           const double* const met[22], double* rh, double* scratch, int sensor,
+                           const double* hybrid_para, cudaStream_t st);
+size_t rhybrid_scratch_doubles(const Grid& g);
+
+// filtering of f for one filter column; scratch >= 2 haloed arrays
+cudaError_t launch_filter(const Grid& g, const Phys& ph, double* f, double* scratch, const double* col,
+                          cudaStream_t st);
+
+// init_mesh on the device: coords (3 haloed arrays, interior filled) -> metrics
+cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* const met[22],
+                        const double periodic_span[3][3], cudaStream_t st);
+
+// show_flow_msg / ana_box partial sums (deterministic two-level reduction)
+cudaError_t launch_flow_msg(const Grid& g, const Phys& ph, const double* f, double* const prim[5],
+                            const double* ajac, double* scratch, double* out3, cudaStream_t st);
+cudaError_t launch_ana_box(const Grid& g, const Phys& ph, const DCoef& dc, double* const prim[5],
+                           const double* const met[22], double* scratch, double* out14, double* out_drms,
+                           cudaStream_t st);
+size_t reduce_scratch_doubles(const Grid& g);
+
+}  // namespace ocfd

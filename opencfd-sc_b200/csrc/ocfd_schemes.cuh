@@ -1,0 +1,298 @@
+// ocfd_schemes.cuh -- point-form upwind reconstructions on a register window.
+//
+// v points at the window element of the face's left point, so v[-3..4] are the
+// stencil values f(i-3..i+4) around face i+1/2.  Each function restates one
+// reference routine operation by operation (no reassociation), so that an
+// FP64 build without FMA contraction reproduces the reference bit for bit;
+// the normal build lets the compiler contract a*b+c into FMAs.
+//
+// R is the arithmetic type: double for the FP64 path, float for the mixed path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ocfd {
+
+template <typename R>
+__device__ __forceinline__ R sq(R x) { return x * x; }
+
+template <typename R>
+__device__ __forceinline__ R sign1(R b) { return copysign(R(1), b); }
+
+template <typename R>
+__device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+template <typename R>
+__device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+
+// hh_weno5P: OCFD_Schemes_1.f90:9-29 (array form OCFD_weno5P, OCFD_Schemes.f90:6-28)
+template <typename R>
+__device__ __forceinline__ R weno5P(const R* v) {
+  const R ep = R(1.0e-6), C03 = R(3.0 / 10.0), C13 = R(3.0 / 5.0), C23 = R(1.0 / 10.0);
+  const R k1312 = R(13.0 / 12.0), k14 = R(1.0 / 4.0);
+  R S0 = k1312 * sq(v[0] - R(2) * v[1] + v[2]) + k14 * sq(R(3) * v[0] - R(4) * v[1] + v[2]);
+  R S1 = k1312 * sq(v[-1] - R(2) * v[0] + v[1]) + k14 * sq(v[-1] - v[1]);
+  R S2 = k1312 * sq(v[-2] - R(2) * v[-1] + v[0]) + k14 * sq(v[-2] - R(4) * v[-1] + R(3) * v[0]);
+  R a0 = C03 / sq(ep + S0);
+  R a1 = C13 / sq(ep + S1);
+  R a2 = C23 / sq(ep + S2);
+  R am = a0 + a1 + a2;
+  R q03 = R(1.0 / 3.0) * v[0] + R(5.0 / 6.0) * v[1] - R(1.0 / 6.0) * v[2];
+  R q13 = R(-1.0 / 6.0) * v[-1] + R(5.0 / 6.0) * v[0] + R(1.0 / 3.0) * v[1];
+  R q23 = R(1.0 / 3.0) * v[-2] - R(7.0 / 6.0) * v[-1] + R(11.0 / 6.0) * v[0];
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+
+// hh_weno5M: OCFD_Schemes_1.f90:31-52 (OCFD_weno5M, OCFD_Schemes.f90:30-53)
+template <typename R>
+__device__ __forceinline__ R weno5M(const R* v) {
+  const R ep = R(1.0e-6), C03 = R(3.0 / 10.0), C13 = R(3.0 / 5.0), C23 = R(1.0 / 10.0);
+  const R k1312 = R(13.0 / 12.0), k14 = R(1.0 / 4.0);
+  R S0 = k1312 * sq(v[1] - R(2) * v[0] + v[-1]) + k14 * sq(R(3) * v[1] - R(4) * v[0] + v[-1]);
+  R S1 = k1312 * sq(v[2] - R(2) * v[1] + v[0]) + k14 * sq(v[2] - v[0]);
+  R S2 = k1312 * sq(v[3] - R(2) * v[2] + v[1]) + k14 * sq(v[3] - R(4) * v[2] + R(3) * v[1]);
+  R a0 = C03 / sq(ep + S0);
+  R a1 = C13 / sq(ep + S1);
+  R a2 = C23 / sq(ep + S2);
+  R am = a0 + a1 + a2;
+  R q03 = R(1.0 / 3.0) * v[1] + R(5.0 / 6.0) * v[0] - R(1.0 / 6.0) * v[-1];
+  R q13 = R(-1.0 / 6.0) * v[2] + R(5.0 / 6.0) * v[1] + R(1.0 / 3.0) * v[0];
+  R q23 = R(1.0 / 3.0) * v[3] - R(7.0 / 6.0) * v[2] + R(11.0 / 6.0) * v[1];
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+
+// hh_weno5P_boundary / hh_weno5M_boundary: OCFD_Schemes_1.f90:266-325.
+// del: 1 = DEL_LIFT, 2 = DEL_RIGHT
+template <typename R>
+__device__ __forceinline__ R weno5P_bnd(const R* v, int del) {
+  const R ep = R(1.0e-6), C03 = R(3.0 / 10.0), C13 = R(3.0 / 5.0), C23 = R(1.0 / 10.0);
+  const R k1312 = R(13.0 / 12.0), k14 = R(1.0 / 4.0);
+  R a0 = R(0), q03 = R(0), a2 = R(0), q23 = R(0);
+  if (del != 2) {
+    R S0 = k1312 * sq(v[0] - R(2) * v[1] + v[2]) + k14 * sq(R(3) * v[0] - R(4) * v[1] + v[2]);
+    a0 = C03 / sq(ep + S0);
+    q03 = R(1.0 / 3.0) * v[0] + R(5.0 / 6.0) * v[1] - R(1.0 / 6.0) * v[2];
+  }
+  R S1 = k1312 * sq(v[-1] - R(2) * v[0] + v[1]) + k14 * sq(v[-1] - v[1]);
+  R a1 = C13 / sq(ep + S1);
+  R q13 = R(-1.0 / 6.0) * v[-1] + R(5.0 / 6.0) * v[0] + R(1.0 / 3.0) * v[1];
+  if (del != 1) {
+    R S2 = k1312 * sq(v[-2] - R(2) * v[-1] + v[0]) + k14 * sq(v[-2] - R(4) * v[-1] + R(3) * v[0]);
+    a2 = C23 / sq(ep + S2);
+    q23 = R(1.0 / 3.0) * v[-2] - R(7.0 / 6.0) * v[-1] + R(11.0 / 6.0) * v[0];
+  }
+  R am = a0 + a1 + a2;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+
+template <typename R>
+__device__ __forceinline__ R weno5M_bnd(const R* v, int del) {
+  const R ep = R(1.0e-6), C03 = R(3.0 / 10.0), C13 = R(3.0 / 5.0), C23 = R(1.0 / 10.0);
+  const R k1312 = R(13.0 / 12.0), k14 = R(1.0 / 4.0);
+  R a0 = R(0), q03 = R(0), a2 = R(0), q23 = R(0);
+  if (del != 1) {
+    R S0 = k1312 * sq(v[1] - R(2) * v[0] + v[-1]) + k14 * sq(R(3) * v[1] - R(4) * v[0] + v[-1]);
+    a0 = C03 / sq(ep + S0);
+    q03 = R(1.0 / 3.0) * v[1] + R(5.0 / 6.0) * v[0] - R(1.0 / 6.0) * v[-1];
+  }
+  R S1 = k1312 * sq(v[2] - R(2) * v[1] + v[0]) + k14 * sq(v[2] - v[0]);
+  R a1 = C13 / sq(ep + S1);
+  R q13 = R(-1.0 / 6.0) * v[2] + R(5.0 / 6.0) * v[1] + R(1.0 / 3.0) * v[0];
+  if (del != 2) {
+    R S2 = k1312 * sq(v[3] - R(2) * v[2] + v[1]) + k14 * sq(v[3] - R(4) * v[2] + R(3) * v[1]);
+    a2 = C23 / sq(ep + S2);
+    q23 = R(1.0 / 3.0) * v[3] - R(7.0 / 6.0) * v[2] + R(11.0 / 6.0) * v[1];
+  }
+  R am = a0 + a1 + a2;
+  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+}
+
+// WENO7 (WENO-JS, 4 candidate stencils): hh_weno7P OCFD_Schemes_1.f90:58-121
+// (array form OCFD_weno7P, OCFD_Schemes.f90:59-124)
+#define OCFD_W7_COEFFS                                                                                 \
+  const R C0 = R(1.0 / 35.0), C1 = R(12.0 / 35.0), C2 = R(18.0 / 35.0), C3 = R(4.0 / 35.0);            \
+  const R a11 = R(-2.0 / 6.0), a12 = R(9.0 / 6.0), a13 = R(-18.0 / 6.0), a14 = R(11.0 / 6.0);          \
+  const R a21 = R(1.0 / 6.0), a23 = R(3.0 / 6.0), a24 = R(2.0 / 6.0);                                  \
+  const R a31 = R(-2.0 / 6.0), a32 = R(-3.0 / 6.0), a34 = R(-1.0 / 6.0);                               \
+  const R a41 = R(-11.0 / 6.0), a42 = R(18.0 / 6.0), a43 = R(-9.0 / 6.0), a44 = R(2.0 / 6.0);          \
+  const R b12 = R(4), b13 = R(-5), b14 = R(2), b22 = R(-2), b41 = R(2), b42 = R(-5), b43 = R(4);        \
+  const R c12 = R(3);                                                                                  \
+  const R d12 = R(13.0 / 12.0), d13 = R(1043.0 / 960.0), d14 = R(1.0 / 12.0);                          \
+  const R e11 = R(-3.0 / 12.0), e12 = R(13.0 / 12.0), e13 = R(-23.0 / 12.0), e14 = R(25.0 / 12.0);     \
+  const R e21 = R(1.0 / 12.0), e22 = R(-5.0 / 12.0), e23 = R(13.0 / 12.0), e24 = R(3.0 / 12.0);        \
+  const R e31 = R(-1.0 / 12.0), e32 = R(7.0 / 12.0), e33 = R(7.0 / 12.0), e34 = R(-1.0 / 12.0);        \
+  const R e41 = R(3.0 / 12.0), e42 = R(13.0 / 12.0), e43 = R(-5.0 / 12.0), e44 = R(1.0 / 12.0);        \
+  const R ep = R(1.0e-8)
+
+template <typename R>
+__device__ __forceinline__ R weno7P(const R* v) {
+  OCFD_W7_COEFFS;
+  R S10 = a11 * v[-3] + a12 * v[-2] + a13 * v[-1] + a14 * v[0];
+  R S11 = a21 * v[-2] - v[-1] + a23 * v[0] + a24 * v[1];
+  R S12 = a31 * v[-1] + a32 * v[0] + v[1] + a34 * v[2];
+  R S13 = a41 * v[0] + a42 * v[1] + a43 * v[2] + a44 * v[3];
+  R S20 = -v[-3] + b12 * v[-2] + b13 * v[-1] + b14 * v[0];
+  R S21 = v[-1] + b22 * v[0] + v[1];
+  R S22 = v[0] + b22 * v[1] + v[2];
+  R S23 = b41 * v[0] + b42 * v[1] + b43 * v[2] - v[3];
+  R S30 = -v[-3] + c12 * (v[-2] - v[-1]) + v[0];
+  R S31 = -v[-2] + c12 * (v[-1] - v[0]) + v[1];
+  R S32 = -v[-1] + c12 * (v[0] - v[1]) + v[2];
+  R S33 = -v[0] + c12 * (v[1] - v[2]) + v[3];
+  R S0 = S10 * S10 + d12 * S20 * S20 + d13 * S30 * S30 + d14 * S10 * S30;
+  R S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
+  R S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
+  R S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
+  R a0 = C0 / sq(ep + S0);
+  R a1 = C1 / sq(ep + S1);
+  R a2 = C2 / sq(ep + S2);
+  R a3 = C3 / sq(ep + S3);
+  R am = a0 + a1 + a2 + a3;
+  R q0 = e11 * v[-3] + e12 * v[-2] + e13 * v[-1] + e14 * v[0];
+  R q1 = e21 * v[-2] + e22 * v[-1] + e23 * v[0] + e24 * v[1];
+  R q2 = e31 * v[-1] + e32 * v[0] + e33 * v[1] + e34 * v[2];
+  R q3 = e41 * v[0] + e42 * v[1] + e43 * v[2] + e44 * v[3];
+  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / am;
+}
+
+// hh_weno7M: OCFD_Schemes_1.f90:124-187 (OCFD_weno7M, OCFD_Schemes.f90:127-193)
+template <typename R>
+__device__ __forceinline__ R weno7M(const R* v) {
+  OCFD_W7_COEFFS;
+  R S10 = a11 * v[4] + a12 * v[3] + a13 * v[2] + a14 * v[1];
+  R S11 = a21 * v[3] - v[2] + a23 * v[1] + a24 * v[0];
+  R S12 = a31 * v[2] + a32 * v[1] + v[0] + a34 * v[-1];
+  R S13 = a41 * v[1] + a42 * v[0] + a43 * v[-1] + a44 * v[-2];
+  R S20 = -v[4] + b12 * v[3] + b13 * v[2] + b14 * v[1];
+  R S21 = v[2] + b22 * v[1] + v[0];
+  R S22 = v[1] + b22 * v[0] + v[-1];
+  R S23 = b41 * v[1] + b42 * v[0] + b43 * v[-1] - v[-2];
+  R S30 = -v[4] + c12 * (v[3] - v[2]) + v[1];
+  R S31 = -v[3] + c12 * (v[2] - v[1]) + v[0];
+  R S32 = -v[2] + c12 * (v[1] - v[0]) + v[-1];
+  R S33 = -v[1] + c12 * (v[0] - v[-1]) + v[-2];
+  R S0 = S10 * S10 + d12 * S20 * S20 + d13 * S30 * S30 + d14 * S10 * S30;
+  R S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
+  R S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
+  R S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
+  R a0 = C0 / sq(ep + S0);
+  R a1 = C1 / sq(ep + S1);
+  R a2 = C2 / sq(ep + S2);
+  R a3 = C3 / sq(ep + S3);
+  R am = a0 + a1 + a2 + a3;
+  R q0 = e11 * v[4] + e12 * v[3] + e13 * v[2] + e14 * v[1];
+  R q1 = e21 * v[3] + e22 * v[2] + e23 * v[1] + e24 * v[0];
+  R q2 = e31 * v[2] + e32 * v[1] + e33 * v[0] + e34 * v[-1];
+  R q3 = e41 * v[1] + e42 * v[0] + e43 * v[-1] + e44 * v[-2];
+  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / am;
+}
+
+// minmod2 / minmod4: OCFD_Schemes.f90:274-289
+template <typename R>
+__device__ __forceinline__ R minmod2(R x1, R x2) {
+  return R(0.5) * (sign1(x1) + sign1(x2)) * rmin(fabs(x1), fabs(x2));
+}
+template <typename R>
+__device__ __forceinline__ R minmod4(R x1, R x2, R x3, R x4) {
+  R r = R(0.5) * (sign1(x1) + sign1(x2));
+  r = r * fabs(R(0.5) * (sign1(x1) + sign1(x3)));
+  r = r * fabs(R(0.5) * (sign1(x1) + sign1(x4)));
+  r = r * rmin(rmin(rmin(fabs(x1), fabs(x2)), fabs(x3)), fabs(x4));
+  return r;
+}
+
+// OMP6 (optimized 6th-order monotonicity-preserving) coefficients,
+// OCFD_Schemes_1.f90:203-209: m = 0.015, n = 0, kappa = 4, and ep = 1.e-10 as a
+// single-precision literal widened to double.
+struct Omp6C {
+  static constexpr double m = 0.015, n = 0.0;
+  static constexpr double a = 0.5 * (m + n), b = 0.5 * (m - n);
+  static constexpr double a1 = a;
+  static constexpr double a2 = 1.0 / 60.0 - b - 6.0 * a;
+  static constexpr double a3 = -2.0 / 15.0 + 6.0 * b + 15.0 * a;
+  static constexpr double a4 = 37.0 / 60.0 - 15.0 * b - 20.0 * a;
+  static constexpr double a5 = 37.0 / 60.0 + 20.0 * b + 15.0 * a;
+  static constexpr double a6 = -2.0 / 15.0 - 6.0 * a - 15.0 * b;
+  static constexpr double a7 = 1.0 / 60.0 + a + 6.0 * b;
+  static constexpr double a8 = -b;
+  static constexpr double kappa = 4.0;
+  static constexpr double ep = (double)1.e-10f;
+};
+
+// The limiter branch of OMP6 (taken rarely in smooth flow), kept out of line
+// so that the common path stays small.  Written for the P orientation
+// (vm2..v2 = v(-2)..v(2)); the M form passes the values mirrored about the face.
+// vlc is the value subtracted in the lc term: v(-1) in hh_OMP6P
+// (OCFD_Schemes_1.f90:219) but v(0) -- not the mirror v(2) -- in hh_OMP6M (:253).
+template <typename R>
+__device__ __noinline__ R omp6_limit(R mid_nf, R vm2, R vm1, R v0, R v1, R v2, R vlc) {
+  const R kappa = R(Omp6C::kappa);
+  R d1 = vm2 + v0 - R(2) * vm1;
+  R d2 = vm1 + v1 - R(2) * v0;
+  R d3 = v0 + v2 - R(2) * v1;
+  R ul = v0 + kappa * (v0 - vm1);
+  R md = R(0.5) * (v0 + v1) - R(0.5) * minmod4(R(4) * d2 - d3, R(4) * d3 - d2, d2, d3);
+  R lc = v0 + R(0.5) * (v0 - vlc) + kappa * minmod4(R(4) * d1 - d2, R(4) * d2 - d1, d2, d1) / R(3);
+  R fmin = rmax(rmin(rmin(v0, v1), md), rmin(rmin(v0, ul), lc));
+  R fmax = rmin(rmax(rmax(v0, v1), md), rmax(rmax(v0, ul), lc));
+  return mid_nf + minmod2(fmax - mid_nf, fmin - mid_nf);
+}
+
+// hh_OMP6P: OCFD_Schemes_1.f90:195-226 (OCFD_OMP6P, OCFD_Schemes.f90:201-234)
+template <typename R>
+__device__ __forceinline__ R omp6P(const R* v) {
+  R mid_nf = R(Omp6C::a1) * v[4] + R(Omp6C::a2) * v[3] + R(Omp6C::a3) * v[2] + R(Omp6C::a4) * v[1] +
+             R(Omp6C::a5) * v[0] + R(Omp6C::a6) * v[-1] + R(Omp6C::a7) * v[-2] + R(Omp6C::a8) * v[-3];
+  R mp = v[0] + minmod2((v[1] - v[0]), R(Omp6C::kappa) * (v[0] - v[-1]));
+  if ((mid_nf - v[0]) * (mid_nf - mp) >= R(Omp6C::ep)) mid_nf = omp6_limit(mid_nf, v[-2], v[-1], v[0], v[1], v[2], v[-1]);
+  return mid_nf;
+}
+
+// hh_OMP6M: OCFD_Schemes_1.f90:228-260 (OCFD_OMP6M, OCFD_Schemes.f90:236-271).
+template <typename R>
+__device__ __forceinline__ R omp6M(const R* v) {
+  R mid_nf = R(Omp6C::a1) * v[-3] + R(Omp6C::a2) * v[-2] + R(Omp6C::a3) * v[-1] + R(Omp6C::a4) * v[0] +
+             R(Omp6C::a5) * v[1] + R(Omp6C::a6) * v[2] + R(Omp6C::a7) * v[3] + R(Omp6C::a8) * v[4];
+  R mp = v[1] + minmod2((v[0] - v[1]), R(Omp6C::kappa) * (v[1] - v[2]));
+  if ((mid_nf - v[1]) * (mid_nf - mp) >= R(Omp6C::ep)) mid_nf = omp6_limit(mid_nf, v[3], v[2], v[1], v[0], v[-1], v[0]);
+  return mid_nf;
+}
+
+// hh_UD7L_P / _M: OCFD_Schemes_1.f90:328-348 (OCFD_UD7L_P/M, OCFD_Schemes.f90:292-316)
+template <typename R>
+__device__ __forceinline__ R ud7lP(const R* U, const R* v) {
+  return U[0] * v[-3] + U[1] * v[-2] + U[2] * v[-1] + U[3] * v[0] + U[4] * v[1] + U[5] * v[2] + U[6] * v[3] +
+         U[7] * v[4];
+}
+template <typename R>
+__device__ __forceinline__ R ud7lM(const R* U, const R* v) {
+  return U[0] * v[4] + U[1] * v[3] + U[2] * v[2] + U[3] * v[1] + U[4] * v[0] + U[5] * v[-1] + U[6] * v[-2] +
+         U[7] * v[-3];
+}
+
+// Scheme ids (OCFD_parameters.f90:23-27)
+enum : int { SCH_WENO5 = 1, SCH_WENO7 = 2, SCH_OMP6 = 3, SCH_UD7L = 4, SCH_HYBRID = 10 };
+
+// Interior scheme of OCFD2d_flux1 / flux_x1 (and the hybrid selection of
+// OCFD_HybridP / hh_HybridP, OCFD_Schemes.f90:319-337, OCFD_Schemes_1.f90:351-365)
+template <int SCHEME, typename R>
+__device__ __forceinline__ R schemeP(const R* v, const R* U, int ihy) {
+  if (SCHEME == SCH_OMP6) return omp6P(v);
+  if (SCHEME == SCH_WENO7) return weno7P(v);
+  if (SCHEME == SCH_WENO5) return weno5P(v);
+  if (SCHEME == SCH_UD7L) return ud7lP(U, v);
+  if (ihy == 1) return ud7lP(U, v);
+  if (ihy == 2) return weno7P(v);
+  return weno5P(v);
+}
+template <int SCHEME, typename R>
+__device__ __forceinline__ R schemeM(const R* v, const R* U, int ihy) {
+  if (SCHEME == SCH_OMP6) return omp6M(v);
+  if (SCHEME == SCH_WENO7) return weno7M(v);
+  if (SCHEME == SCH_WENO5) return weno5M(v);
+  if (SCHEME == SCH_UD7L) return ud7lM(U, v);
+  if (ihy == 1) return ud7lM(U, v);
+  if (ihy == 2) return weno7M(v);
+  return weno5M(v);
+}
+
+}  // namespace ocfd

@@ -1,0 +1,222 @@
+"""Host-side mirror of OpenCFD-SC's solver interface over the C ABI.
+
+``Solver`` exposes the reference's hot-path subroutines under their own names
+(exchange_boundary_xyz, comput_Rhybrid, du_inviscous, du_inviscous_Character,
+du_viscous, OCFD_time_adv_RK3, comput_duvwT, OCFD_bc, filtering) with the same
+argument meaning and call order as NS_solver (OCFD_NS_Solver.f90:21-78), plus
+``step`` -- the fused, CUDA-graph-captured equivalent of one pass of the time
+loop.  Errors are raised, matching the reference's print-and-stop: more than
+10 negative-temperature points raise NegativeTemperatureStop.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .params import LAP, N_METRICS, PRECISION_MIXED, SCHEME_HYBRID, OcfdParams
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_parameters(p: OcfdParams, strict: bool = False) -> OcfdParams:
+    """set_parameters (OCFD_readpara.f90:261-341) through the library."""
+    q = p.copy()
+    r = _lib.lib(strict).ocfd_set_parameters(C.byref(q))
+    if r != 0:
+        raise _lib.OcfdError(r, "unsupported configuration")
+    return q
+
+
+def footprint(p: OcfdParams) -> int:
+    return int(_lib.lib().ocfd_gpu_footprint(C.byref(p)))
+
+
+class Solver:
+    def __init__(self, p: OcfdParams, device: int = 0, strict: bool = False):
+        self.L = _lib.lib(strict)
+        self.p = set_parameters(p, strict)
+        self.nx, self.ny, self.nz = self.p.nx, self.p.ny, self.p.nz
+        self.shape_h = (self.nz + 2 * LAP, self.ny + 2 * LAP, self.nx + 2 * LAP)
+        self.shape5 = (5, self.nz, self.ny, self.nx)
+        h = C.c_void_p()
+        r = self.L.ocfd_gpu_create(C.byref(self.p), device, C.byref(h))
+        if r != 0:
+            raise _lib.OcfdError(r, f"ocfd_gpu_create failed (device {device})")
+        self.h = h
+
+    # ------------------------------------------------------------------ plumbing
+    def _check(self, r: int, what: str):
+        if r == 0:
+            return
+        msg = self.L.ocfd_gpu_last_error(self.h)
+        msg = msg.decode() if msg else ""
+        if r == _lib.OCFD_E_NEGT:
+            raise _lib.NegativeTemperatureStop(r, msg or what)
+        raise _lib.OcfdError(r, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ocfd_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.ocfd_gpu_stream(self.h) or 0)
+
+    def sync(self):
+        self._check(self.L.ocfd_gpu_sync(self.h), "sync")
+
+    # ------------------------------------------------------------------ init (init3d)
+    def init_mesh(self, x=None, y=None, z=None):
+        """init_mesh (OCFD_mesh.f90:1-58) on the device; None -> mesh_gen('box')."""
+        if x is None:
+            self._check(self.L.ocfd_gpu_init_mesh(self.h, None, None, None), "init_mesh")
+        else:
+            xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+            self._check(self.L.ocfd_gpu_init_mesh(self.h, _dp(xs[0]), _dp(xs[1]), _dp(xs[2])), "init_mesh")
+
+    def upload_metrics(self, metrics):
+        ms = [np.ascontiguousarray(m, dtype=np.float64) for m in metrics]
+        arr = (C.POINTER(C.c_double) * 22)(*[_dp(m) for m in ms])
+        self._check(self.L.ocfd_gpu_upload_metrics(self.h, arr), "upload_metrics")
+
+    def download_metrics(self):
+        ms = [np.empty(self.shape_h) for _ in range(N_METRICS)]
+        arr = (C.POINTER(C.c_double) * 22)(*[_dp(m) for m in ms])
+        self._check(self.L.ocfd_gpu_download_metrics(self.h, arr), "download_metrics")
+        return ms
+
+    def init3d(self, prims, istep: int = 0, tt: float = 0.0):
+        """init3d (OCFD_init.f90:1-20) from interior primitives + OCFD_bc (OCFD_NS_Solver.f90:15)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in prims]
+        ptrs = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in arrs])
+        self._check(self.L.ocfd_gpu_init3d(self.h, ptrs, istep, tt), "init3d")
+
+    def upload_state(self, f=None, prims_haloed=None, istep=0, tt=0.0):
+        fa = None if f is None else np.ascontiguousarray(f, dtype=np.float64)
+        pp = None
+        keep = []
+        if prims_haloed is not None:
+            keep = [np.ascontiguousarray(a, dtype=np.float64) for a in prims_haloed]
+            pp = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in keep])
+        self._check(self.L.ocfd_gpu_upload_state(self.h, None if fa is None else _dp(fa),
+                                                 None if pp is None else C.cast(pp, C.c_void_p), istep, tt),
+                    "upload_state")
+
+    # ------------------------------------------------------------------ downloads
+    def download_state(self):
+        f = np.empty(self.shape5)
+        prims = [np.empty(self.shape_h) for _ in range(5)]
+        pp = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in prims])
+        self._check(self.L.ocfd_gpu_download_state(self.h, _dp(f), C.cast(pp, C.c_void_p)), "download_state")
+        return f, prims
+
+    def download_f(self):
+        f = np.empty(self.shape5)
+        self._check(self.L.ocfd_gpu_download_state(self.h, _dp(f), None), "download_state")
+        return f
+
+    def download_du(self):
+        du = np.empty(self.shape5)
+        self._check(self.L.ocfd_gpu_download_du(self.h, _dp(du)), "download_du")
+        return du
+
+    def download_rhybrid(self):
+        rh = np.empty(self.shape_h)
+        self._check(self.L.ocfd_gpu_download_rhybrid(self.h, _dp(rh)), "download_rhybrid")
+        return rh
+
+    def time(self):
+        i = C.c_int()
+        t = C.c_double()
+        self._check(self.L.ocfd_gpu_get_time(self.h, C.byref(i), C.byref(t)), "get_time")
+        return i.value, t.value
+
+    # ------------------------------------------------------------------ the reference's subroutines
+    def save_fn(self):
+        self._check(self.L.ocfd_gpu_save_fn(self.h), "save_fn")
+
+    def exchange_boundary_xyz(self):
+        """exchange_boundary_xyz(d,u,v,w,T) (OCFD_NS_Solver.f90:35-39)."""
+        self._check(self.L.ocfd_gpu_halo_prims(self.h), "exchange_boundary_xyz")
+
+    def comput_Rhybrid(self):
+        self._check(self.L.ocfd_gpu_rhybrid(self.h), "comput_Rhybrid")
+
+    def du_inviscous(self):
+        self._check(self.L.ocfd_gpu_du_inviscous(self.h), "du_inviscous")
+
+    def du_inviscous_Character(self):
+        self._check(self.L.ocfd_gpu_du_inviscous_character(self.h), "du_inviscous_Character")
+
+    def du_viscous(self):
+        self._check(self.L.ocfd_gpu_du_viscous(self.h), "du_viscous")
+
+    def OCFD_time_adv_RK3(self, krk: int):
+        self._check(self.L.ocfd_gpu_rk3(self.h, krk), "OCFD_time_adv_RK3")
+
+    def comput_duvwT(self) -> int:
+        n = C.c_int()
+        self._check(self.L.ocfd_gpu_duvwt(self.h, C.byref(n)), "comput_duvwT")
+        return n.value
+
+    def OCFD_bc(self):
+        self._check(self.L.ocfd_gpu_bc(self.h), "OCFD_bc")
+
+    def filtering(self):
+        self._check(self.L.ocfd_gpu_filter(self.h), "filtering")
+
+    def stage_step(self):
+        """One pass of the time loop through the stage operators, in the
+        reference's call order (OCFD_NS_Solver.f90:23-67)."""
+        self.save_fn()
+        for krk in (1, 2, 3):
+            self.exchange_boundary_xyz()
+            if krk == 1 and self.p.scheme_invis == SCHEME_HYBRID:
+                self.comput_Rhybrid()
+            if self.p.if_scheme_character == 0:
+                self.du_inviscous()
+            else:
+                self.du_inviscous_Character()
+            if self.p.if_viscous == 1:
+                self.du_viscous()
+            self.OCFD_time_adv_RK3(krk)
+            self.comput_duvwT()
+            self.OCFD_bc()
+        self._check(self.L.ocfd_gpu_advance_clock(self.h), "advance_clock")
+        self.filtering()
+
+    def step(self, n: int = 1, sync: bool = True):
+        """n time steps on the fused, graph-captured path."""
+        self._check(self.L.ocfd_gpu_step(self.h, n, 1 if sync else 0), "step")
+
+    # ------------------------------------------------------------------ diagnostics
+    def show_flow_msg(self) -> np.ndarray:
+        e = np.zeros(3)
+        self._check(self.L.ocfd_gpu_show_flow_msg(self.h, _dp(e)), "show_flow_msg")
+        return e
+
+    def ana_box(self) -> np.ndarray:
+        e = np.zeros(20)
+        self._check(self.L.ocfd_gpu_ana_box(self.h, _dp(e)), "ana_box")
+        return e
+
+    @property
+    def mixed(self) -> bool:
+        return self.p.precision == PRECISION_MIXED

@@ -1,0 +1,242 @@
+"""GPU parity against the CPU oracle, through the C ABI.
+
+Two builds of the library run every case:
+  strict (-fmad=false): every FP64 operation in the reference's order without
+    FMA contraction -> the result must be bit-identical to the oracle;
+  fast (FMA contraction): the production build -> within tolerance:
+    du of one stage 1e-10 relative to max|du| (du is a difference of face
+    fluxes about 200x larger than du itself at Ma 0.1, so FMA-level rounding
+    of the fluxes shows up amplified), the state after N steps 1e-12 relative
+    L2 (the stated FP64 bar for a full run is 1e-10).
+The sensor-2 hybrid case uses a parallel reduction for the domain mean and is
+compared with tolerance in both builds.
+"""
+import numpy as np
+import pytest
+
+from ocfd_testlib import curvilinear_case, interior, rel_err, rel_l2, tgv_case
+from ocfd_b200.params import (BC_BLUNT2D, BC_USER_DEF, SCHEME_HYBRID, SCHEME_OMP6, SCHEME_UD7L, SCHEME_WENO5,
+                              SCHEME_WENO7, SPLIT_LLF, SPLIT_SW)
+from ocfd_b200.solver import Solver
+from pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TGV_CASES = {
+    "weno7_sw": dict(scheme=SCHEME_WENO7, character=0),
+    "weno7_sw_char": dict(scheme=SCHEME_WENO7, character=1),
+    "omp6_sw_char": dict(scheme=SCHEME_OMP6, character=1),
+    "omp6_sw": dict(scheme=SCHEME_OMP6, character=0),
+    "weno5_llf": dict(scheme=SCHEME_WENO5, character=0, split=SPLIT_LLF),
+    "weno5_llf_char": dict(scheme=SCHEME_WENO5, character=1, split=SPLIT_LLF),
+    "ud7l_sw_cd8": dict(scheme=SCHEME_UD7L, character=0, cd8=True),
+    "hybrid1_llf": dict(scheme=SCHEME_HYBRID, character=0, split=SPLIT_LLF, ma=0.5),
+    "hybrid1_sw_char": dict(scheme=SCHEME_HYBRID, character=1, ma=0.5),
+}
+
+
+def _pair(p, mesh, prims, strict):
+    o = Oracle(p)
+    if mesh is None:
+        o.init_mesh()
+    else:
+        o.init_mesh(*mesh)
+    o.init3d(prims)
+    s = Solver(p, strict=strict)
+    if mesh is None:
+        s.init_mesh()
+    else:
+        s.init_mesh(*mesh)
+    s.init3d(prims)
+    return o, s
+
+
+def _check(a, b, strict, tol):
+    if strict:
+        np.testing.assert_array_equal(a, b)
+    else:
+        assert rel_err(a, b) <= tol, rel_err(a, b)
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "fast"])
+def test_metrics_device_init_box(strict):
+    p, mesh, prims = tgv_case()
+    o, s = _pair(p, mesh, prims, strict)
+    mg = s.download_metrics()
+    for m in range(22):
+        _check(interior(mg[m]), interior(o.metric(m)), strict, 1e-13)
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "fast"])
+@pytest.mark.parametrize("name", list(TGV_CASES))
+def test_rhs_one_stage(name, strict):
+    """du of one stage (du_inviscous[_Character] + du_viscous) against the oracle."""
+    p, mesh, prims = tgv_case(**TGV_CASES[name])
+    o, s = _pair(p, mesh, prims, strict)
+    for x in (o, s):
+        if isinstance(x, Oracle):
+            x.halo_prims()
+        else:
+            x.exchange_boundary_xyz()
+        if p.scheme_invis == SCHEME_HYBRID:
+            x.comput_rhybrid() if isinstance(x, Oracle) else x.comput_Rhybrid()
+        if p.if_scheme_character:
+            x.du_inviscous_character() if isinstance(x, Oracle) else x.du_inviscous_Character()
+        else:
+            x.du_inviscous()
+    du_inv = s.download_du()
+    _check(du_inv, o.du, strict, 1e-10)
+    o.du_viscous()
+    s.du_viscous()
+    _check(s.download_du(), o.du, strict, 1e-10)
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "fast"])
+@pytest.mark.parametrize("name", ["weno7_sw", "omp6_sw_char", "hybrid1_sw_char", "weno5_llf"])
+def test_steps_fused(name, strict):
+    """3 full time steps on the fused graph path against the oracle's NS_solver loop."""
+    p, mesh, prims = tgv_case(**TGV_CASES[name])
+    o, s = _pair(p, mesh, prims, strict)
+    o.step(3)
+    s.step(3)
+    f, pr = s.download_state()
+    if strict:
+        np.testing.assert_array_equal(f, o.f)
+        for q in range(5):
+            np.testing.assert_array_equal(interior(pr[q]), interior(o.prim(q)))
+    else:
+        assert rel_l2(f, o.f) < 1e-12
+    assert s.time()[0] == 3
+
+
+@pytest.mark.parametrize("name", ["weno7_sw", "omp6_sw_char"])
+def test_stage_api_equals_fused(name):
+    """The reference-order stage operators and the fused step give the same bits."""
+    p, mesh, prims = tgv_case(**TGV_CASES[name])
+    a = Solver(p)
+    b = Solver(p)
+    for s in (a, b):
+        s.init_mesh()
+        s.init3d(prims)
+    a.stage_step()
+    a.stage_step()
+    b.step(2)
+    fa, pa = a.download_state()
+    fb, pb = b.download_state()
+    np.testing.assert_array_equal(fa, fb)
+    for q in range(5):
+        np.testing.assert_array_equal(interior(pa[q]), interior(pb[q]))
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "fast"])
+@pytest.mark.parametrize("bc,ghost,scheme,character",
+                         [(BC_USER_DEF, True, SCHEME_WENO7, 1), (BC_BLUNT2D, False, SCHEME_WENO5, 1),
+                          (BC_USER_DEF, True, SCHEME_WENO7, 0), (BC_BLUNT2D, False, SCHEME_OMP6, 0)],
+                         ids=["user_ghost_w7_char", "blunt_w5_char", "user_ghost_w7", "blunt_omp6"])
+def test_curvilinear_boundaries(bc, ghost, scheme, character, strict):
+    """Body-fitted 2-D plane grid, non-periodic i/j with boundary closures, wall BC,
+    ghost cells, periodic span: metrics, one RHS and 3 steps."""
+    p, mesh, prims = curvilinear_case(bc=bc, ghost=ghost, scheme=scheme, character=character)
+    o, s = _pair(p, mesh, prims, strict)
+    mg = s.download_metrics()
+    for m in range(22):
+        _check(mg[m][4:-4, :, :], o.metric(m)[4:-4, :, :], strict, 1e-12)
+    f0, _ = s.download_state()
+    _check(f0, o.f, strict, 1e-14)
+    o.step(3)
+    s.step(3)
+    f, pr = s.download_state()
+    if strict:
+        np.testing.assert_array_equal(f, o.f)
+    else:
+        assert rel_l2(f, o.f) < 1e-11
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "fast"])
+def test_hybrid_sensor2(strict):
+    p, mesh, prims = tgv_case(scheme=SCHEME_HYBRID, character=1, sensor=2, t1=0.5, t2=1.5, ma=0.5)
+    o, s = _pair(p, mesh, prims, strict)
+    o.halo_prims()
+    s.exchange_boundary_xyz()
+    o.comput_rhybrid()
+    s.comput_Rhybrid()
+    assert rel_err(interior(s.download_rhybrid()), interior(o.rhybrid)) < 1e-13
+    o.step(2)
+    s.step(2)
+    assert rel_l2(s.download_f(), o.f) < 1e-11
+
+
+@pytest.mark.parametrize("scheme_f", [1, 2], ids=["fo9p", "shock"])
+def test_filtering(scheme_f):
+    p, mesh, prims = tgv_case(scheme=SCHEME_WENO7)
+    p.nfiltering = 1
+    col = p.filter_para[0]
+    col[0] = 1  # every step
+    col[1] = col[2] = col[3] = 1
+    col[4], col[5], col[6], col[7], col[8], col[9] = 1, 1000, 1, 1000, 1, 1000
+    col[10] = scheme_f
+    col[11] = 1.0
+    col[12] = 1e-5
+    o, s = _pair(p, mesh, prims, True)
+    o.step(2)
+    s.step(2)
+    np.testing.assert_array_equal(s.download_f(), o.f)
+
+
+def test_negative_temperature_repair():
+    """Host-planted negative energy at a few points: comput_duvwT repairs them in the
+    reference's sweep order (6-neighbour mean, new values before, old after)."""
+    p, mesh, prims = tgv_case()
+    o, s = _pair(p, mesh, prims, True)
+    f = o.f.copy()
+    pts = [(3, 4, 5), (3, 4, 6), (10, 2, 7), (5, 5, 5)]  # (k, j, i) zero-based, two neighbours
+    for (k, j, i) in pts:
+        f[4, k, j, i] = 0.3 * (f[1, k, j, i] ** 2 + f[2, k, j, i] ** 2 + f[3, k, j, i] ** 2) / f[0, k, j, i]
+    o.f[...] = f
+    s.upload_state(f=f)
+    o.halo_prims()
+    s.exchange_boundary_xyz()
+    n_o = o.duvwt()
+    n_s = s.comput_duvwT()
+    assert n_o == n_s == len(pts)
+    _, pr = s.download_state()
+    for q in range(5):
+        np.testing.assert_array_equal(interior(pr[q]), interior(o.prim(q)))
+
+
+def test_negative_temperature_stop():
+    from ocfd_b200._lib import NegativeTemperatureStop
+
+    p, mesh, prims = tgv_case()
+    o, s = _pair(p, mesh, prims, True)
+    f = s.download_f()
+    f[4, 2, 2, 2:14] = 0.0  # 12 points with T < 0
+    s.upload_state(f=f)
+    with pytest.raises(NegativeTemperatureStop):
+        s.comput_duvwT()
+
+
+def test_diagnostics():
+    p, mesh, prims = tgv_case()
+    o, s = _pair(p, mesh, prims, True)
+    o.step(1)
+    s.step(1)
+    assert rel_err(s.show_flow_msg(), o.show_flow_msg()) < 1e-13
+    a, b = s.ana_box(), o.ana_box()
+    assert rel_err(a[1:], b[1:]) < 1e-10
+
+
+def test_mixed_precision_close_to_fp64():
+    p, mesh, prims = tgv_case(scheme=SCHEME_OMP6, character=1)
+    pm, _, _ = tgv_case(scheme=SCHEME_OMP6, character=1, mixed=True)
+    a = Solver(p)
+    b = Solver(pm)
+    for s in (a, b):
+        s.init_mesh()
+        s.init3d(prims)
+    a.step(5)
+    b.step(5)
+    fa, fb = a.download_f(), b.download_f()
+    assert rel_l2(fb, fa) < 1e-6
+    ea, eb = a.show_flow_msg(), b.show_flow_msg()
+    assert abs(eb[1] - ea[1]) / ea[1] < 1e-6

@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark of the OpenCFD-SC RHS + RK3 hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tgv256_omp6_char] [--precision fp64|mixed]
+
+One "step" is one RK3 time step (three stages) of the whole grid.  The
+default workload is the Taylor-Green vortex on a 256^3 periodic box with the
+characteristic flux path and OMP6, FP64 (the reference's du_inviscous_Character
++ du_viscous + OCFD_time_adv_RK3 + comput_duvwT + OCFD_bc per stage).  The
+stated dt of 0.002 is above the stability limit of RK3 with these schemes at
+Ma 0.1 on 256^3 (acoustic CFL 0.9 per direction; the oracle stops with the
+reference's negative-temperature error after 17 steps at that CFL, and after 21
+steps at dt = 0.001 for the characteristic OMP6 path); dt = 0.0005 (CFL 0.22)
+is used.  The metric does not depend on dt.
+
+Multi-GPU: the path does not shard in this build (one grid per GPU); N GPUs run
+N independent replicas ("replicas only", weak scaling), the time is the max
+over ranks and the value is the total grid-point updates of all ranks.
+
+--impl reference times the CPU restatement of the reference (the oracle, all
+host threads via OpenMP) on the same configuration; each of its steps is one
+time step of a 128^3 sample of the workload (1/8 of the points).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "opencfd-sc_b200"))
+
+METRIC = "grid-pt RK3 updates/s FP64 vs mixed at stated L2 err; served p50/p99 latency"
+UNIT = "GPts/s"
+
+WORKLOADS = {
+    # name: (grid, scheme, character, split, dt, description)
+    "tgv256_omp6_char": (256, "OMP6", 1, 1, 0.0005, "Taylor-Green vortex 256^3, characteristic flux, OMP6, SW, CD6"),
+    "tgv256_hybrid_char": (256, "HYBRID", 1, 1, 0.0005, "Taylor-Green vortex 256^3, characteristic flux, hybrid UD7L(CD8)/WENO7/WENO5, SW"),
+    "tgv64_weno7": (64, "WENO7", 0, 1, 0.005, "Taylor-Green vortex 64^3, flux-vector form, WENO7, SW, CD6"),
+    "tgv256_weno7": (256, "WENO7", 0, 1, 0.0005, "Taylor-Green vortex 256^3, flux-vector form, WENO7, SW, CD6"),
+}
+
+
+def make_params(workload: str, precision: str, n_override: int | None = None):
+    from ocfd_b200 import cases
+    from ocfd_b200.params import SCHEME
+
+    n, scheme, chr_, split, dt, _ = WORKLOADS[workload]
+    if n_override:
+        n = n_override
+    p = cases.tgv_params(n, scheme=SCHEME[scheme], character=chr_, split=split, dt=dt)
+    if scheme == "HYBRID":
+        p.hybrid_para[0] = 1
+        p.hybrid_para[1] = 0.004
+        p.hybrid_para[2] = 0.01
+        p.ud7l_diss = 0.0
+    p.precision = 1 if precision == "mixed" else 0
+    return p
+
+
+# ---------------------------------------------------------------------------------------------
+# byte model (algorithmic bytes per grid point, per launch) of each kernel group
+def byte_model(p) -> dict:
+    r = 4 if p.precision == 1 else 8  # face fluxes / Ev / FP32 copies of prims+metrics
+    s = 4 if p.precision == 1 else 8  # prims + metric rows read by the face kernels
+    nface = 5 if p.if_scheme_character else 10
+    face = 8 * s + nface * r  # d,u,v,w,T + 3 metric rows in; faces out
+    visc = 4 * s + 18 * s + 12 * r  # u,v,w,T + 18 metrics in; 12 Ev out
+    # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out
+    tail = 3 * nface * r + 12 * r + 8 + 40 + 40 * 2.0 / 3.0 + 40 + 40 + (20 if p.precision == 1 else 0)
+    return {"face_x": face, "face_y": face, "face_z": face, "visc_grad": visc, "stage_tail": tail}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """dram bytes per grid point per launch from the committed ncu summaries (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+            sm = [float(r[1]) for r in rows if len(r) >= 9]
+            mx = [float(r[2]) for r in rows if len(r) >= 9]
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                if len(r) < 9:
+                    continue
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            if sm:
+                out["sm_mhz"] = statistics.median(sm)
+                out["sm_max_mhz"] = max(mx)
+                out["samples"] = len(sm)
+            out["reasons"] = sorted(reasons)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        return out
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_rate(p, steps: int, warm: int = 1):
+    """Oracle (CPU restatement, OpenMP over the host cores) grid-point updates per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+
+    from ocfd_b200 import cases
+
+    o = Oracle(p)
+    o.init_mesh()
+    o.init3d(cases.tgv_prims(o.p))
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    n = p.nx * p.ny * p.nz
+    o.close()
+    return n * steps / dt / 1e9, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing
+
+    cores = multiprocessing.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    wl = WORKLOADS[args.workload]
+    nsample = min(wl[0], 128)
+    p = make_params(args.workload, "fp64", n_override=nsample)
+    rate, secs = cpu_rate(p, args.steps, warm=args.warmup)
+    ms = secs / args.steps * 1e3 * (wl[0] ** 3) / (nsample ** 3)
+    sample = (f"{args.steps} time steps of TGV {nsample}^3 (same scheme; {nsample ** 3} of the workload's "
+              f"{wl[0] ** 3} points per step) after {args.warmup} warm-up steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
+        "config": {"workload": args.workload, "description": wl[5], "grid": f"{wl[0]}^3", "sample_grid": f"{nsample}^3"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if dist:
+        import datetime
+
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    from ocfd_b200 import cases
+    from ocfd_b200.solver import Solver
+
+    p = make_params(args.workload, args.precision)
+    n = p.nx * p.ny * p.nz
+    s = Solver(p, device=local)
+    s.init_mesh()
+    s.init3d(cases.tgv_prims(s.p))
+    stream = torch.cuda.ExternalStream(s.stream, device=local)
+
+    s.step(args.warmup, sync=True)  # includes graph capture
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.step(args.steps, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    s.sync()
+    value = world * n * args.steps / (ms * 1e-3) / 1e9
+    clocks = clk.summary()
+
+    # kernels launched per step on the fused path
+    per_stage = 3 + (1 if p.if_viscous else 0) + 2
+    launches = args.steps * (3 * per_stage + (1 if p.scheme_invis == 10 else 0))
+
+    # ---- per-kernel timing (roofline of the dominant kernel)
+    prof = s.profile_steps(3)
+    model = byte_model(s.p)
+    groups = {k: v for k, v in prof.items() if k in model}
+    dom = max(groups, key=groups.get)
+    t_launch = groups[dom] / 3.0 * 1e-3  # 3 launches per step
+    achieved = model[dom] * n / t_launch / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic().get(f"{args.workload}:{args.precision}:{dom}")
+
+    # ---- end to end through the C ABI with host-owned state: per step, upload
+    # f + haloed primitives from pinned host memory, one time step, download them.
+    K2 = max(1, min(args.steps, 5))
+    f_host = torch.empty(s.shape5, dtype=torch.float64, pin_memory=True).numpy()
+    prim_host = [torch.empty(s.shape_h, dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+    import ctypes as C
+
+    L = s.L
+    dp = C.POINTER(C.c_double)
+    fptr = f_host.ctypes.data_as(dp)
+    parr = (dp * 5)(*[a.ctypes.data_as(dp) for a in prim_host])
+    L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
+    istep, tt = s.time()
+    if dist:
+        tdist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K2):
+        L.ocfd_gpu_upload_state(s.h, fptr, C.cast(parr, C.c_void_p), istep, tt)
+        L.ocfd_gpu_step(s.h, 1, 0)
+        L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * n * K2 / t_e2e / 1e9
+    bytes_state = 5 * 8 * (n + int(np.prod(s.shape_h)))
+    s.sync()  # raises if the run hit the reference's negative-temperature stop
+    ke = s.show_flow_msg()[1]
+    if not np.isfinite(ke):
+        raise RuntimeError("non-finite kinetic energy: the run is invalid")
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu and world == 1:
+            import multiprocessing
+
+            cores = multiprocessing.cpu_count()
+            os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+            nsample = min(p.nx, 128)
+            pc = make_params(args.workload, "fp64", n_override=nsample)
+            rate, secs = cpu_rate(pc, 3)
+            cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+                   "sample": f"3 time steps of TGV {nsample}^3 with the same scheme on the oracle ({secs:.1f} s)"}
+        wl = WORKLOADS[args.workload]
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state",
+            "data": "synthetic (analytic Taylor-Green initial field)",
+            "config": {"workload": args.workload, "description": wl[5], "grid": f"{p.nx}^3", "dt": p.dt,
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state of a 256^3 grid is GBs)"},
+            "clocks": clocks,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state,
+                    "mode": "host-owned state: upload f + primitives, one step, download f + primitives"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind, "bytes_per_point": model[dom],
+                         "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()}},
+            "cpu_baseline": cpu,
+            "kinetic_energy": ke,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tgv256_omp6_char", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -243,6 +243,15 @@ int ocfd_gpu_advance_clock(ocfd_handle* h);
  * the next synchronous call (and by this one when sync != 0). */
 int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync);
 
+/* Run nsteps fused steps eagerly (no graph) with CUDA events around each kernel
+ * group on the instance's stream; ms[] receives the average milliseconds per
+ * step of: [0] shock sensor, [1] x faces, [2] y faces, [3] z faces, [4]
+ * viscous gradients, [5] fused stage tail, [6] negative-T repair + BC +
+ * halos, [7] the whole step.  Advances the solution like ocfd_gpu_step.
+ * (Timing instrumentation: the reference only times the whole loop with
+ * MPI_wtime, OCFD_NS_Solver.f90:18-19,79-80.) */
+int ocfd_gpu_profile_steps(ocfd_handle* h, int nsteps, double ms[8]);
+
 /* ---------------------------------------------------------------------------
  * Diagnostics on the device
  * ------------------------------------------------------------------------- */

@@ -46,9 +46,15 @@ struct ocfd_handle {
   double* dout = nullptr;      // small device output block
   double* hout = nullptr;      // pinned
   double** dptr = nullptr;     // device pointer table (halo lists)
-  // graphs: one step, for each parity of the (f,fn) and T buffer pairs
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  int parity = 0;
+  // captured one-step graphs, keyed by the buffer assignment they were
+  // captured with: (f, fn) order x (T, second T) order -> at most 4
+  struct GraphSlot {
+    double* f;
+    double* fn;
+    double* t;
+    cudaGraphExec_t g;
+  } graphs[4] = {};
+  int ngraphs = 0;
   bool halo_valid = false;
   bool metrics_ready = false;
   int istep = 0;
@@ -261,6 +267,7 @@ void* ocfd_gpu_stream(ocfd_handle* h) { return h ? (void*)h->st : nullptr; }
 int ocfd_gpu_sync(ocfd_handle* h) {
   if (!h) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->hstat, h->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   if (h->hstat->error == 3)
     return fail(h, OCFD_E_NEGT, "Number of Negative Temperature Points >  Limit, STOP !");
@@ -271,8 +278,8 @@ void ocfd_gpu_destroy(ocfd_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->st) cudaStreamSynchronize(h->st);
-  for (int q = 0; q < 2; q++)
-    if (h->gexec[q]) cudaGraphExecDestroy(h->gexec[q]);
+  for (int q = 0; q < h->ngraphs; q++)
+    if (h->graphs[q].g) cudaGraphExecDestroy(h->graphs[q].g);
   auto F = [](void* p) {
     if (p) cudaFree(p);
   };
@@ -559,9 +566,10 @@ int ocfd_gpu_rhybrid(ocfd_handle* h) {
 }  // extern "C"
 
 template <typename R, typename S>
-static int faces(ocfd_handle* h) {
+static int faces(ocfd_handle* h, int dsel = -1) {
   const Grid& g = h->g;
   for (int d = 0; d < 3; d++) {
+    if (dsel >= 0 && d != dsel) continue;
     FaceArgs<S> a;
     a.g = g;
     a.ph = h->ph;
@@ -754,18 +762,41 @@ int ocfd_gpu_advance_clock(ocfd_handle* h) {
 }
 
 // ------------------------------------------------------------------ fused step
+// Optional per-kernel timing of the fused path: events recorded on the
+// instance's stream around each kernel group.
+struct Prof {
+  cudaEvent_t ev[16];
+  int n = 0;
+  int group[16];
+};
+static void prof_mark(ocfd_handle* h, Prof* pf, int group) {
+  if (!pf || pf->n >= 16) return;
+  pf->group[pf->n] = group;
+  cudaEventRecord(pf->ev[pf->n++], h->st);
+}
+
 // One RK stage of NS_solver (OCFD_NS_Solver.f90:35-58) on the fused path.
-static int fused_stage(ocfd_handle* h, int krk) {
+// Timing groups: 0 sensor, 1-3 face x/y/z, 4 viscous gradients, 5 stage tail,
+// 6 negative-T repair + BC + halos.
+static int fused_stage(ocfd_handle* h, int krk, Prof* pf = nullptr) {
+  prof_mark(h, pf, 0);
   if (krk == 1 && h->p.scheme_invis == OCFD_SCHEME_HYBRID) {
     int r = ocfd_gpu_rhybrid(h);
     if (r) return r;
   }
-  int r = h->mixed ? faces<float, float>(h) : faces<double, double>(h);
-  if (r) return r;
-  if (h->p.if_viscous) {
-    r = h->mixed ? visc_grad<float, float>(h) : visc_grad<double, double>(h);
+  const Grid& g = h->g;
+  for (int d = 0; d < 3; d++) {
+    prof_mark(h, pf, 1 + d);
+    int r = h->mixed ? faces<float, float>(h, d) : faces<double, double>(h, d);
     if (r) return r;
   }
+  (void)g;
+  prof_mark(h, pf, 4);
+  if (h->p.if_viscous) {
+    int r = h->mixed ? visc_grad<float, float>(h) : visc_grad<double, double>(h);
+    if (r) return r;
+  }
+  prof_mark(h, pf, 5);
   if (h->mixed) {
     UpdArgs<float> a = upd_args<float>(h);
     a.krk = krk;
@@ -777,6 +808,7 @@ static int fused_stage(ocfd_handle* h, int krk) {
     a.du = nullptr;
     CK(launch_fused<double>(a, h->st));
   }
+  prof_mark(h, pf, 6);
   UpdArgs<double> fx = upd_args<double>(h);
   CK(launch_negt_fix(fx, h->st));
   swap_t(h);
@@ -784,20 +816,66 @@ static int fused_stage(ocfd_handle* h, int krk) {
     CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
     CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
     CK(launch_ghost(h->g, h->ph, h->prim, h->st));
-    r = halo_all(h);
+    int r = halo_all(h);
     if (r) return r;
     r = refresh_p32(h);
     if (r) return r;
   }
+  prof_mark(h, pf, 7);
   return OCFD_OK;
 }
 
-static int fused_step(ocfd_handle* h) {
+static int fused_step(ocfd_handle* h, Prof* pf = nullptr, double* acc = nullptr) {
   std::swap(h->f, h->fn);  // fn = f (stage 1 overwrites all of f)
   for (int krk = 1; krk <= 3; krk++) {
-    int r = fused_stage(h, krk);
+    if (pf) pf->n = 0;
+    int r = fused_stage(h, krk, pf);
     if (r) return r;
+    if (pf) {
+      CK(cudaEventSynchronize(pf->ev[pf->n - 1]));
+      for (int q = 0; q + 1 < pf->n; q++) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, pf->ev[q], pf->ev[q + 1]));
+        acc[pf->group[q]] += ms;
+      }
+    }
   }
+  return OCFD_OK;
+}
+
+extern "C" int ocfd_gpu_profile_steps(ocfd_handle* h, int nsteps, double ms[8]) {
+  if (!h || nsteps <= 0 || !ms) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (!h->halo_valid) {
+    int r = halo_all(h);
+    if (r) return r;
+    h->halo_valid = true;
+  }
+  Prof pf;
+  for (int q = 0; q < 16; q++) CK(cudaEventCreate(&pf.ev[q]));
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  double tot = 0.0;
+  int r = OCFD_OK;
+  for (int s = 0; s < nsteps && r == OCFD_OK; s++) {
+    CK(cudaEventRecord(t0, h->st));
+    r = fused_step(h, &pf, acc);
+    CK(cudaEventRecord(t1, h->st));
+    CK(cudaEventSynchronize(t1));
+    float mt = 0.f;
+    CK(cudaEventElapsedTime(&mt, t0, t1));
+    tot += mt;
+    h->istep += 1;
+    h->tt += h->p.dt;
+  }
+  for (int q = 0; q < 16; q++) cudaEventDestroy(pf.ev[q]);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (r) return r;
+  for (int q = 0; q < 7; q++) ms[q] = acc[q] / nsteps;
+  ms[7] = tot / nsteps;
   return OCFD_OK;
 }
 
@@ -815,9 +893,12 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
       int r = fused_step(h);
       if (r) return r;
     } else {
-      const int par = h->parity;
-      if (!h->gexec[par]) {
-        // eager run of this parity once (sets kernel attributes), then capture
+      ocfd_handle::GraphSlot* slot = nullptr;
+      for (int q = 0; q < h->ngraphs; q++)
+        if (h->graphs[q].f == h->f && h->graphs[q].fn == h->fn && h->graphs[q].t == h->prim[4]) slot = &h->graphs[q];
+      if (!slot) {
+        // capture one step with the current buffer assignment (capture does
+        // not execute; the host-side pointer swaps are undone afterwards)
         double* f0 = h->f;
         double* fn0 = h->fn;
         double* t0 = h->prim[4];
@@ -826,22 +907,25 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
         int r = fused_step(h);
         cudaError_t e = cudaStreamEndCapture(h->st, &graph);
-        if (r) return r;
-        if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&h->gexec[par], graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
-        // capture does not execute: restore the pointers and run the graph
         h->f = f0;
         h->fn = fn0;
         h->prim[4] = t0;
         h->talt = ta0;
+        if (r) return r;
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+        slot = &h->graphs[h->ngraphs];
+        e = cudaGraphInstantiate(&slot->g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+        slot->f = f0;
+        slot->fn = fn0;
+        slot->t = t0;
+        h->ngraphs++;
       }
-      CK(cudaGraphLaunch(h->gexec[par], h->st));
+      CK(cudaGraphLaunch(slot->g, h->st));
+      // the step swaps (f, fn) once and the temperature buffers three times
       std::swap(h->f, h->fn);
-      // three T swaps per step = one net swap
       std::swap(h->prim[4], h->talt);
-      h->parity ^= 1;
     }
     h->istep += 1;
     h->tt += h->p.dt;
@@ -850,10 +934,7 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
       if (r) return r;
     }
   }
-  if (sync) {
-    CK(cudaMemcpyAsync(h->hstat, h->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->st));
-    return ocfd_gpu_sync(h);
-  }
+  if (sync) return ocfd_gpu_sync(h);
   return OCFD_OK;
 }
 

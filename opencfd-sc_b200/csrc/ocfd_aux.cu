@@ -40,7 +40,7 @@ __global__ void k_final_sum(const double* part, int nb, double* out) {
 }
 
 // central derivative of a haloed FP64 array (OCFD_dx0/dy0/dz0)
-__device__ __noinline__ double d0h_bnd(const double* q, long long s, int l, int nn, int cd8, const DCoef& c, int dir) {
+__device__ __forceinline__ double d0h_bnd(const double* q, long long s, int l, int nn, int cd8, const DCoef& c, int dir) {
   auto at = [&](int off) -> double { return q[off * s]; };
   const double h = c.h[dir], a1 = c.a1[dir], a2 = c.a2[dir], a3 = c.a3[dir];
   double r = 0.0;

@@ -1,4 +1,4 @@
-// ocfd_face.cu -- face-flux kernels of the inviscous terms, one launch per
+// ocfd_face.cuh -- face-flux kernels of the inviscous terms, one launch per
 // direction: split -> (characteristic projection) -> reconstruction, written
 // as numerical fluxes h(i+1/2) per face.  The flux difference, the Jacobian
 // scaling and the rest of the stage happen in the update kernel
@@ -16,6 +16,7 @@
 // Phase 2 computes one face per thread from a register window of 8 points.
 // For a periodic direction face 0 equals face n bit for bit, so only faces
 // 1..n are computed: n faces for n points, no tile does extra work.
+#pragma once
 #include <cstring>
 
 #include "ocfd_device.cuh"
@@ -181,8 +182,12 @@ struct Stencil<SCH_WENO5> {
 };
 
 // ---------------------------------------------------------------------------
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
-__global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
+// ALLIN: every face of the launch is an interior face (periodic direction), so
+// the boundary-closure paths are compiled out.
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
+// FP64: two resident blocks per SM (<= 128 registers) measured faster than one;
+// FP32 needs fewer registers and is faster without the cap.
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S> a) {
   constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
   // shared memory: 10 split-flux arrays (+7 face-state arrays for CHAR)
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -195,7 +200,7 @@ __global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
   int g0, pbase;
   if (DIR == 0) {
     g0 = a.fbeg + blockIdx.x * TF;
-    pbase = blockIdx.y * NP;
+    pbase = blockIdx.y * NP;  // NP consecutive j of plane k = blockIdx.z + 1
   } else {
     g0 = a.fbeg + blockIdx.y * TF;
     pbase = blockIdx.x * NP;
@@ -203,11 +208,10 @@ __global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
   // pencil p -> (i,j,k) with the along-direction index left at 0
   auto pencil = [&](int p, int& i, int& j, int& k) -> bool {
     if (DIR == 0) {
-      int pen = pbase + p;
       i = 0;
-      j = pen % G.ny + 1;
-      k = pen / G.ny + 1;
-      return pen < G.ny * G.nz;
+      j = pbase + p + 1;
+      k = blockIdx.z + 1;
+      return j <= G.ny;
     } else if (DIR == 1) {
       i = pbase + p + 1;
       j = 0;
@@ -277,6 +281,8 @@ __global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
 #pragma unroll
   for (int q = 0; q < 8; q++) U[q] = R(ph.ud7l[q]);
   R* out = reinterpret_cast<R*>(a.hh);
+  // window element (var, stencil offset s) of this thread's face at wb[var*VS + (s+3)*QS]
+  constexpr int VS = NP * LT, QS = DIR == 0 ? 1 : NP;
 
   for (int t = threadIdx.x; t < NP * TF; t += blockDim.x) {
     int f, p;
@@ -291,6 +297,8 @@ __global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
     if (!pencil(p, i, j, k)) continue;
     const int g = g0 + f;
     if (g > a.fend) continue;
+    const R* wb = sm + (DIR == 0 ? p * LT + f : f * NP + p);
+    auto W = [&](int var, int q) -> R { return wb[var * VS + q * QS]; };
     int ii = DIR == 0 ? g : i, jj = DIR == 1 ? g : j, kk = DIR == 2 ? g : k;
     const long long fo = G.face(DIR, g, ii, jj, kk);
     int ihy = 0;
@@ -306,173 +314,244 @@ __global__ void __launch_bounds__(256) k_face(FaceArgs<S> a) {
       // ---- flux-vector form: h1 (F+) and h2 (F-) per variable
       const int ib1 = (bi0 == 0 || sb0 == -1) ? 0 : -ph.ka1 + 1, ie1 = (bi1 == 0 || sb1 == -1) ? nn : nn - ph.kb1;
       const int ib2 = (bi0 == 0 || sb0 == -1) ? 0 : -ph.ka2 + 1, ie2 = (bi1 == 0 || sb1 == -1) ? nn : nn - ph.kb2;
-      const bool inner = g >= ib1 && g <= ie1 && g >= ib2 && g <= ie2;
+      const bool inner = ALLIN || (g >= ib1 && g <= ie1 && g >= ib2 && g <= ie2);
+      if (inner) {
+#pragma unroll 1
+        for (int m = 0; m < 5; m++) {
+          R wv[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) wv[q] = W(m, q);
+          const R h1 = schemeP<SCHEME>(wv + 3, U, ihy);
+#pragma unroll
+          for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
+          const R h2 = schemeM<SCHEME>(wv + 3, U, ihy);
+          out[fo + (long long)m * a.fs] = h1;
+          out[fo + (long long)(5 + m) * a.fs] = h2;
+        }
+      } else if (!ALLIN) {
+#pragma unroll 1
+        for (int m = 0; m < 5; m++) {
+          R wv[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) wv[q] = W(m, q);
+          const R h1 = nc_flux1_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
+#pragma unroll
+          for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
+          const R h2 = nc_flux2_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
+          out[fo + (long long)m * a.fs] = h1;
+          out[fo + (long long)(5 + m) * a.fs] = h2;
+        }
+      }
+      continue;
+    }
+
+    // ---- characteristic form (flux_charteric)
+    const int ia = (bi0 == 0 || sb0 != 0) ? 0 : 1;
+    const int ibf = (bi1 == 0 || sb1 != 0) ? nn : nn - 1;
+    R hh[5];
+    if (!ALLIN && (g < ia || g > ibf)) {
+      // non-reflecting boundary faces, OCFD_inviscous_character.f90:295-309
 #pragma unroll 1
       for (int m = 0; m < 5; m++) {
-        R wv[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) wv[q] = sm[SI(m, f + q, p)];
-        R h1 = inner ? schemeP<SCHEME>(wv + 3, U, ihy) : nc_flux1_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
-#pragma unroll
-        for (int q = 0; q < 8; q++) wv[q] = sm[SI(5 + m, f + q, p)];
-        R h2 = inner ? schemeM<SCHEME>(wv + 3, U, ihy) : nc_flux2_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
-        out[fo + (long long)m * a.fs] = h1;
-        out[fo + (long long)(5 + m) * a.fs] = h2;
+        if (g == 0)
+          hh[m] = (R(2) * W(m, 4) + R(5) * W(m, 5) - W(m, 6) + R(2) * W(5 + m, 6) - R(7) * W(5 + m, 5) +
+                   R(11) * W(5 + m, 4)) / R(6);
+        else
+          hh[m] = (R(2) * W(m, 1) - R(7) * W(m, 2) + R(11) * W(m, 3) + R(2) * W(5 + m, 3) + R(5) * W(5 + m, 2) -
+                   W(5 + m, 1)) / R(6);
       }
     } else {
-      // ---- characteristic form (flux_charteric)
-      const int ia = (bi0 == 0 || sb0 != 0) ? 0 : 1;
-      const int ibf = (bi1 == 0 || sb1 != 0) ? nn : nn - 1;
-      R hh[5];
-      if (g < ia || g > ibf) {
-        // non-reflecting boundary faces, OCFD_inviscous_character.f90:295-309
-#pragma unroll
+      const bool inner1 =
+          ALLIN || ((bi0 == 0 || g > -ph.ka1 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb1 || sb1 == -1));
+      const bool inner2 =
+          ALLIN || ((bi0 == 0 || g > -ph.ka2 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb2 || sb1 == -1));
+      const bool inner = inner1 && inner2;
+      if (ihy == 1) {
+        // linear hybrid face: no characteristic projection (:192-194, :281-282)
+#pragma unroll 1
         for (int m = 0; m < 5; m++) {
-          R fpv[8], fmv[8];
+          R wv[8];
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
-            fpv[q] = sm[SI(m, f + q, p)];
-            fmv[q] = sm[SI(5 + m, f + q, p)];
-          }
-          const R* P = fpv + 3;
-          const R* M = fmv + 3;
-          if (g == 0)
-            hh[m] = (R(2) * P[1] + R(5) * P[2] - P[3] + R(2) * M[3] - R(7) * M[2] + R(11) * M[1]) / R(6);
-          else
-            hh[m] = (R(2) * P[-2] - R(7) * P[-1] + R(11) * P[0] + R(2) * M[0] + R(5) * M[-1] - M[-2]) / R(6);
+          for (int q = 0; q < 8; q++) wv[q] = W(m, q);
+          const R h1 = (ALLIN || inner) ? schemeP<SCHEME>(wv + 3, U, ihy) : ch_flux1_bnd(wv + 3, g, nn, ph, DIR);
+#pragma unroll
+          for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
+          const R h2 = (ALLIN || inner) ? schemeM<SCHEME>(wv + 3, U, ihy) : ch_flux2_bnd(wv + 3, g, nn, ph, DIR);
+          hh[m] = h1 + h2;
         }
       } else {
-        const bool inner1 = (bi0 == 0 || g > -ph.ka1 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb1 || sb1 == -1);
-        const bool inner2 = (bi0 == 0 || g > -ph.ka2 || sb0 == -1) && (bi1 == 0 || g <= nn - ph.kb2 || sb1 == -1);
-        if (ihy == 1) {
-          // linear hybrid face: no characteristic projection (:192-194, :281-282)
-#pragma unroll 1
-          for (int m = 0; m < 5; m++) {
-            R wv[8];
+        // face state: arithmetic means of the two neighbours (:205-211)
+        const R u1 = (W(10, 3) + W(10, 4)) * R(0.5);
+        const R v1 = (W(11, 3) + W(11, 4)) * R(0.5);
+        const R w1 = (W(12, 3) + W(12, 4)) * R(0.5);
+        const R c1 = (W(13, 3) + W(13, 4)) * R(0.5);
+        const R a1 = (W(14, 3) + W(14, 4)) * R(0.5);
+        const R a2 = (W(15, 3) + W(15, 4)) * R(0.5);
+        const R a3 = (W(16, 3) + W(16, 4)) * R(0.5);
+        // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
+        R ss = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
+        const R n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
+        R l1, l2, l3;
+        if (fabs(n3) <= fabs(n2)) {
+          ss = sqrt(n1 * n1 + n2 * n2);
+          l1 = -n2 / ss;
+          l2 = n1 / ss;
+          l3 = R(0);
+        } else {
+          ss = sqrt(n1 * n1 + n3 * n3);
+          l1 = -n3 / ss;
+          l2 = R(0);
+          l3 = n1 / ss;
+        }
+        const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+        const R un = u1 * n1 + v1 * n2 + w1 * n3;
+        const R ul = u1 * l1 + v1 * l2 + w1 * l3;
+        const R um = u1 * m1 + v1 * m2 + w1 * m3;
+        const R V2 = (u1 * u1 + v1 * v1 + w1 * w1) * R(0.5);
+        const R KK = (R(ph.gamma) - R(1)) / (c1 * c1);
+        const R KK1 = KK * R(0.5);
+        const R X1 = R(1) / (R(2) * c1);
+        const R L[5][5] = {{R(1) - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
+                           {-ul, l1, l2, l3, R(0)},
+                           {-um, m1, m2, m3, R(0)},
+                           {KK1 * V2 + X1 * un, -X1 * n1 - KK1 * u1, -X1 * n2 - KK1 * v1, -X1 * n3 - KK1 * w1, KK1},
+                           {KK1 * V2 - X1 * un, X1 * n1 - KK1 * u1, X1 * n2 - KK1 * v1, X1 * n3 - KK1 * w1, KK1}};
+        // projection of one stencil point (:256-260 / :266-270), row r
+        auto proj_row = [&](int r, int vb, int q) -> R {
+          const R f0 = W(vb, q), f1 = W(vb + 1, q), f2 = W(vb + 2, q), f3 = W(vb + 3, q);
+          if (r == 1 || r == 2) return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3;
+          return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3 + L[r][4] * W(vb + 4, q);
+        };
+        R h0[5];
+        if (SCHEME == SCH_OMP6 && inner) {
+          // OMP6, interior face: the linear part of hh_OMP6P/M (OCFD_Schemes_1.f90:211,244) is
+          // accumulated while the stencil is projected point by point, in the
+          // reference's term order; only v(-1..1) (F+) / v(0..2) (F-) are kept for
+          // the monotonicity test, the two outer values are recomputed in the
+          // (rare) limiter branch.
+          const R oa[8] = {R(Omp6C::a1), R(Omp6C::a2), R(Omp6C::a3), R(Omp6C::a4),
+                           R(Omp6C::a5), R(Omp6C::a6), R(Omp6C::a7), R(Omp6C::a8)};
+          const R kap = R(Omp6C::kappa), ep = R(Omp6C::ep);
+          {
+            R mid[5], vm1[5], v0[5], vp1[5];
 #pragma unroll
-            for (int q = 0; q < 8; q++) wv[q] = sm[SI(m, f + q, p)];
-            R h1 = inner1 ? schemeP<SCHEME>(wv + 3, U, ihy) : ch_flux1_bnd(wv + 3, g, nn, ph, DIR);
+            for (int s = 4; s >= -3; s--) {
+              const int q = s + 3;
+              const R f0 = W(0, q), f1 = W(1, q), f2 = W(2, q), f3 = W(3, q), f4 = W(4, q);
+              R c[5];
+              c[0] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
+              c[1] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
+              c[2] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
+              c[3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
+              c[4] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
 #pragma unroll
-            for (int q = 0; q < 8; q++) wv[q] = sm[SI(5 + m, f + q, p)];
-            R h2 = inner2 ? schemeM<SCHEME>(wv + 3, U, ihy) : ch_flux2_bnd(wv + 3, g, nn, ph, DIR);
-            hh[m] = h1 + h2;
+              for (int r = 0; r < 5; r++) {
+                mid[r] = (s == 4) ? oa[0] * c[r] : mid[r] + oa[4 - s] * c[r];
+                if (s == -1) vm1[r] = c[r];
+                if (s == 0) v0[r] = c[r];
+                if (s == 1) vp1[r] = c[r];
+              }
+            }
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              const R mp = v0[r] + minmod2((vp1[r] - v0[r]), kap * (v0[r] - vm1[r]));
+              if ((mid[r] - v0[r]) * (mid[r] - mp) >= ep) {
+                const R vm2 = proj_row(r, 0, 1), vp2 = proj_row(r, 0, 5);
+                mid[r] = omp6_limit(mid[r], vm2, vm1[r], v0[r], vp1[r], vp2, vm1[r]);
+              }
+              h0[r] = mid[r];
+            }
+          }
+          {
+            R mid[5], v0[5], v1[5], v2[5];
+#pragma unroll
+            for (int s = -3; s <= 4; s++) {
+              const int q = s + 3;
+              const R f0 = W(5, q), f1 = W(6, q), f2 = W(7, q), f3 = W(8, q), f4 = W(9, q);
+              R c[5];
+              c[0] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
+              c[1] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
+              c[2] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
+              c[3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
+              c[4] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
+#pragma unroll
+              for (int r = 0; r < 5; r++) {
+                mid[r] = (s == -3) ? oa[0] * c[r] : mid[r] + oa[s + 3] * c[r];
+                if (s == 0) v0[r] = c[r];
+                if (s == 1) v1[r] = c[r];
+                if (s == 2) v2[r] = c[r];
+              }
+            }
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              const R mp = v1[r] + minmod2((v0[r] - v1[r]), kap * (v1[r] - v2[r]));
+              if ((mid[r] - v1[r]) * (mid[r] - mp) >= ep) {
+                const R v3 = proj_row(r, 5, 6), vm1 = proj_row(r, 5, 2);
+                mid[r] = omp6_limit(mid[r], v3, v2[r], v1[r], v0[r], vm1, v0[r]);
+              }
+              h0[r] = h0[r] + mid[r];
+            }
           }
         } else {
-          // face state: arithmetic means of the two neighbours (:205-211)
-          const int sL = f + 3, sR = f + 4;
-          const R u1 = (sm[SI(10, sL, p)] + sm[SI(10, sR, p)]) * R(0.5);
-          const R v1 = (sm[SI(11, sL, p)] + sm[SI(11, sR, p)]) * R(0.5);
-          const R w1 = (sm[SI(12, sL, p)] + sm[SI(12, sR, p)]) * R(0.5);
-          const R c1 = (sm[SI(13, sL, p)] + sm[SI(13, sR, p)]) * R(0.5);
-          const R a1 = (sm[SI(14, sL, p)] + sm[SI(14, sR, p)]) * R(0.5);
-          const R a2 = (sm[SI(15, sL, p)] + sm[SI(15, sR, p)]) * R(0.5);
-          const R a3 = (sm[SI(16, sL, p)] + sm[SI(16, sR, p)]) * R(0.5);
-          // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
-          R ss = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
-          const R n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
-          R l1, l2, l3;
-          if (fabs(n3) <= fabs(n2)) {
-            ss = sqrt(n1 * n1 + n2 * n2);
-            l1 = -n2 / ss;
-            l2 = n1 / ss;
-            l3 = R(0);
-          } else {
-            ss = sqrt(n1 * n1 + n3 * n3);
-            l1 = -n3 / ss;
-            l2 = R(0);
-            l3 = n1 / ss;
-          }
-          const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
-          const R un = u1 * n1 + v1 * n2 + w1 * n3;
-          const R ul = u1 * l1 + v1 * l2 + w1 * l3;
-          const R um = u1 * m1 + v1 * m2 + w1 * m3;
-          const R V2 = (u1 * u1 + v1 * v1 + w1 * w1) * R(0.5);
-          const R KK = (R(ph.gamma) - R(1)) / (c1 * c1);
-          const R KK1 = KK * R(0.5);
-          const R X1 = R(1) / (R(2) * c1);
-          const R L[5][5] = {{R(1) - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
-                             {-ul, l1, l2, l3, R(0)},
-                             {-um, m1, m2, m3, R(0)},
-                             {KK1 * V2 + X1 * un, -X1 * n1 - KK1 * u1, -X1 * n2 - KK1 * v1, -X1 * n3 - KK1 * w1, KK1},
-                             {KK1 * V2 - X1 * un, X1 * n1 - KK1 * u1, X1 * n2 - KK1 * v1, X1 * n3 - KK1 * w1, KK1}};
-          R h0[5];
           // ---- F+ projected onto the characteristic variables (:254-261), reconstructed
           {
             R q[5][8];
             constexpr int LO = Stencil<SCHEME>::PLO, HI = Stencil<SCHEME>::PHI;
 #pragma unroll
-            for (int s = LO; s <= HI; s++) {
-              const int l = f + 3 + s;
-              const R f0 = sm[SI(0, l, p)], f1 = sm[SI(1, l, p)], f2 = sm[SI(2, l, p)], f3 = sm[SI(3, l, p)],
-                      f4 = sm[SI(4, l, p)];
-              q[0][s + 3] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
-              q[1][s + 3] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
-              q[2][s + 3] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
-              q[3][s + 3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
-              q[4][s + 3] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
-            }
-#pragma unroll
             for (int s = -3; s <= 4; s++)
-              if (s < LO || s > HI)
 #pragma unroll
-                for (int r = 0; r < 5; r++) q[r][s + 3] = R(0);
+              for (int r = 0; r < 5; r++) q[r][s + 3] = (s < LO || s > HI) ? R(0) : proj_row(r, 0, s + 3);
+            if (ALLIN || inner1) {
 #pragma unroll
-            for (int r = 0; r < 5; r++)
-              h0[r] = inner1 ? schemeP<SCHEME>(q[r] + 3, U, ihy) : ch_flux1_bnd(q[r] + 3, g, nn, ph, DIR);
+              for (int r = 0; r < 5; r++) h0[r] = schemeP<SCHEME>(q[r] + 3, U, ihy);
+            } else {
+#pragma unroll
+              for (int r = 0; r < 5; r++) h0[r] = ch_flux1_bnd(q[r] + 3, g, nn, ph, DIR);
+            }
           }
           // ---- F- (:264-271)
           {
             R q[5][8];
             constexpr int LO = Stencil<SCHEME>::MLO, HI = Stencil<SCHEME>::MHI;
 #pragma unroll
-            for (int s = LO; s <= HI; s++) {
-              const int l = f + 3 + s;
-              const R f0 = sm[SI(5, l, p)], f1 = sm[SI(6, l, p)], f2 = sm[SI(7, l, p)], f3 = sm[SI(8, l, p)],
-                      f4 = sm[SI(9, l, p)];
-              q[0][s + 3] = L[0][0] * f0 + L[0][1] * f1 + L[0][2] * f2 + L[0][3] * f3 + L[0][4] * f4;
-              q[1][s + 3] = L[1][0] * f0 + L[1][1] * f1 + L[1][2] * f2 + L[1][3] * f3;
-              q[2][s + 3] = L[2][0] * f0 + L[2][1] * f1 + L[2][2] * f2 + L[2][3] * f3;
-              q[3][s + 3] = L[3][0] * f0 + L[3][1] * f1 + L[3][2] * f2 + L[3][3] * f3 + L[3][4] * f4;
-              q[4][s + 3] = L[4][0] * f0 + L[4][1] * f1 + L[4][2] * f2 + L[4][3] * f3 + L[4][4] * f4;
-            }
-#pragma unroll
             for (int s = -3; s <= 4; s++)
-              if (s < LO || s > HI)
 #pragma unroll
-                for (int r = 0; r < 5; r++) q[r][s + 3] = R(0);
+              for (int r = 0; r < 5; r++) q[r][s + 3] = (s < LO || s > HI) ? R(0) : proj_row(r, 5, s + 3);
+            if (ALLIN || inner2) {
 #pragma unroll
-            for (int r = 0; r < 5; r++) {
-              R h2 = inner2 ? schemeM<SCHEME>(q[r] + 3, U, ihy) : ch_flux2_bnd(q[r] + 3, g, nn, ph, DIR);
-              h0[r] = h0[r] + h2;
+              for (int r = 0; r < 5; r++) h0[r] = h0[r] + schemeM<SCHEME>(q[r] + 3, U, ihy);
+            } else {
+#pragma unroll
+              for (int r = 0; r < 5; r++) h0[r] = h0[r] + ch_flux2_bnd(q[r] + 3, g, nn, ph, DIR);
             }
           }
-          // ---- back to physical space, hh = R h0 (:284-288); R = S^-1 (:244-248)
-          const R H = V2 + R(1) / KK;
-          hh[0] = h0[0] + h0[3] + h0[4];
-          hh[1] = u1 * h0[0] + l1 * h0[1] + m1 * h0[2] + (u1 - c1 * n1) * h0[3] + (u1 + c1 * n1) * h0[4];
-          hh[2] = v1 * h0[0] + l2 * h0[1] + m2 * h0[2] + (v1 - c1 * n2) * h0[3] + (v1 + c1 * n2) * h0[4];
-          hh[3] = w1 * h0[0] + l3 * h0[1] + m3 * h0[2] + (w1 - c1 * n3) * h0[3] + (w1 + c1 * n3) * h0[4];
-          hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - c1 * un) * h0[3] + (H + c1 * un) * h0[4];
         }
+        // ---- back to physical space, hh = R h0 (:284-288); R = S^-1 (:244-248)
+        const R H = V2 + R(1) / KK;
+        hh[0] = h0[0] + h0[3] + h0[4];
+        hh[1] = u1 * h0[0] + l1 * h0[1] + m1 * h0[2] + (u1 - c1 * n1) * h0[3] + (u1 + c1 * n1) * h0[4];
+        hh[2] = v1 * h0[0] + l2 * h0[1] + m2 * h0[2] + (v1 - c1 * n2) * h0[3] + (v1 + c1 * n2) * h0[4];
+        hh[3] = w1 * h0[0] + l3 * h0[1] + m3 * h0[2] + (w1 - c1 * n3) * h0[3] + (w1 + c1 * n3) * h0[4];
+        hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - c1 * un) * h0[3] + (H + c1 * un) * h0[4];
       }
-#pragma unroll
-      for (int m = 0; m < 5; m++) out[fo + (long long)m * a.fs] = hh[m];
     }
+#pragma unroll
+    for (int m = 0; m < 5; m++) out[fo + (long long)m * a.fs] = hh[m];
   }
 }
 
 // ---------------------------------------------------------------------------
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
 static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
   constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
   constexpr int NV = CHAR ? 17 : 10;  // split fluxes (+ face state)
   const size_t smem = (size_t)NV * NP * LT * sizeof(R);
-  auto kern = k_face<DIR, CHAR, SCHEME, R, S>;
+  auto kern = k_face<DIR, CHAR, SCHEME, ALLIN, R, S>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int nf = a.fend - a.fbeg + 1;
   dim3 grid;
   if (DIR == 0) {
-    grid = dim3((nf + TF - 1) / TF, (a.g.ny * a.g.nz + NP - 1) / NP, 1);
+    grid = dim3((nf + TF - 1) / TF, (a.g.ny + NP - 1) / NP, a.g.nz);
   } else {
     grid = dim3((a.g.nx + NP - 1) / NP, (nf + TF - 1) / TF, DIR == 1 ? a.g.nz : a.g.ny);
   }
@@ -482,8 +561,10 @@ static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
 
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st) {
-#define OCFD_FACE_CASE(D, C, SC) \
-  if (dir == D && chr == C && scheme == SC) return launch_face_t<D, C, SC, R, S>(a, st);
+  const bool allin = a.ph.periodic[dir] != 0;
+#define OCFD_FACE_CASE(D, C, SC)                                                    \
+  if (dir == D && chr == C && scheme == SC)                                         \
+    return allin ? launch_face_t<D, C, SC, true, R, S>(a, st) : launch_face_t<D, C, SC, false, R, S>(a, st);
 #define OCFD_FACE_SCHEMES(D, C)         \
   OCFD_FACE_CASE(D, C, SCH_WENO5)       \
   OCFD_FACE_CASE(D, C, SCH_WENO7)       \
@@ -499,28 +580,6 @@ cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cud
 #undef OCFD_FACE_SCHEMES
 #undef OCFD_FACE_CASE
   return cudaErrorInvalidValue;
-}
-
-template cudaError_t launch_face<double, double>(int, bool, int, const FaceArgs<double>&, cudaStream_t);
-template cudaError_t launch_face<float, float>(int, bool, int, const FaceArgs<float>&, cudaStream_t);
-
-// A FaceArgs with an empty grid asks launch_face_t to set the kernel's
-// shared-memory attribute instead of launching it.
-cudaError_t setup_face_kernels() {
-  const int schemes[5] = {SCH_WENO5, SCH_WENO7, SCH_OMP6, SCH_UD7L, SCH_HYBRID};
-  FaceArgs<double> ad;
-  FaceArgs<float> af;
-  memset(&ad, 0, sizeof(ad));
-  memset(&af, 0, sizeof(af));
-  for (int d = 0; d < 3; d++)
-    for (int c = 0; c < 2; c++)
-      for (int s = 0; s < 5; s++) {
-        cudaError_t e = launch_face<double, double>(d, c == 1, schemes[s], ad, 0);
-        if (e != cudaSuccess) return e;
-        e = launch_face<float, float>(d, c == 1, schemes[s], af, 0);
-        if (e != cudaSuccess) return e;
-      }
-  return cudaSuccess;
 }
 
 }  // namespace ocfd

@@ -17,34 +17,42 @@ namespace ocfd {
 // Central derivatives OCFD_dx0/dy0/dz0 (OCFD_dxyz_viscous.f90:3-239) of a
 // pencil given by an accessor at(off) = q(l+off).  Interior CD6/CD8 and the
 // low-order closures of a non-periodic boundary.
+// Coefficients of one direction, by value (no reference into the kernel's
+// parameter block, which would force it into local memory).
+template <typename R>
+struct D0C {
+  R h, a1, a2, a3, c1, c2, c3, c4;
+};
+template <typename R>
+__device__ __forceinline__ D0C<R> d0c(const DCoef& c, int dir) {
+  return D0C<R>{R(c.h[dir]), R(c.a1[dir]), R(c.a2[dir]), R(c.a3[dir]),
+                R(c.c1[dir]), R(c.c2[dir]), R(c.c3[dir]), R(c.c4[dir])};
+}
+
 // Closures only: called for l in {1,2,3,(4)} or {(n-3),n-2,n-1,n}, never reads
 // outside 1..n along the direction (the Ev arrays carry no halo).
 template <typename R, typename F>
-__device__ __noinline__ R d0_bnd(F at, int l, int nn, int cd8, const DCoef& c, int dir) {
-  const R h = R(c.h[dir]);
-  const R a1 = R(c.a1[dir]), a2 = R(c.a2[dir]), a3 = R(c.a3[dir]);
+__device__ __forceinline__ R d0_bnd(F at, int l, int nn, int cd8, D0C<R> k) {
   R r = R(0);
-  if (l == 1) r = (R(-3) * at(0) + R(4) * at(1) - at(2)) / (R(2) * h);
-  else if (l == 2) r = (at(1) - at(-1)) / (R(2) * h);
-  else if (l == 3) r = (R(8) * (at(1) - at(-1)) - (at(2) - at(-2))) / (R(12) * h);
-  else if (cd8 && l == 4) r = a1 * (at(3) - at(-3)) + a2 * (at(2) - at(-2)) + a3 * (at(1) - at(-1));
-  if (l == nn) r = (at(-2) - R(4) * at(-1) + R(3) * at(0)) / (R(2) * h);
-  else if (l == nn - 1) r = (at(1) - at(-1)) / (R(2) * h);
-  else if (l == nn - 2) r = (R(8) * (at(1) - at(-1)) - (at(2) - at(-2))) / (R(12) * h);
-  else if (cd8 && l == nn - 3) r = a1 * (at(3) - at(-3)) + a2 * (at(2) - at(-2)) + a3 * (at(1) - at(-1));
+  if (l == 1) r = (R(-3) * at(0) + R(4) * at(1) - at(2)) / (R(2) * k.h);
+  else if (l == 2) r = (at(1) - at(-1)) / (R(2) * k.h);
+  else if (l == 3) r = (R(8) * (at(1) - at(-1)) - (at(2) - at(-2))) / (R(12) * k.h);
+  else if (cd8 && l == 4) r = k.a1 * (at(3) - at(-3)) + k.a2 * (at(2) - at(-2)) + k.a3 * (at(1) - at(-1));
+  if (l == nn) r = (at(-2) - R(4) * at(-1) + R(3) * at(0)) / (R(2) * k.h);
+  else if (l == nn - 1) r = (at(1) - at(-1)) / (R(2) * k.h);
+  else if (l == nn - 2) r = (R(8) * (at(1) - at(-1)) - (at(2) - at(-2))) / (R(12) * k.h);
+  else if (cd8 && l == nn - 3) r = k.a1 * (at(3) - at(-3)) + k.a2 * (at(2) - at(-2)) + k.a3 * (at(1) - at(-1));
   return r;
 }
 
 template <typename R, typename F>
-__device__ __forceinline__ R d0(F at, int l, int nn, int periodic, int cd8, const DCoef& c, int dir) {
+__device__ __forceinline__ R d0(F at, int l, int nn, int periodic, int cd8, D0C<R> k) {
   const int lo = cd8 ? 4 : 3, hi = cd8 ? nn - 3 : nn - 2;
   if (periodic || (l > lo && l < hi)) {
-    if (!cd8)
-      return R(c.a1[dir]) * (at(3) - at(-3)) + R(c.a2[dir]) * (at(2) - at(-2)) + R(c.a3[dir]) * (at(1) - at(-1));
-    return R(c.c1[dir]) * (at(1) - at(-1)) + R(c.c2[dir]) * (at(2) - at(-2)) + R(c.c3[dir]) * (at(3) - at(-3)) +
-           R(c.c4[dir]) * (at(4) - at(-4));
+    if (!cd8) return k.a1 * (at(3) - at(-3)) + k.a2 * (at(2) - at(-2)) + k.a3 * (at(1) - at(-1));
+    return k.c1 * (at(1) - at(-1)) + k.c2 * (at(2) - at(-2)) + k.c3 * (at(3) - at(-3)) + k.c4 * (at(4) - at(-4));
   }
-  return d0_bnd<R>(at, l, nn, cd8, c, dir);
+  return d0_bnd<R>(at, l, nn, cd8, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -69,7 +77,7 @@ __global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
       const long long hs = G.hstride(dir);
       const S* base = q4[q] + c;
       auto at = [&](int off) -> R { return R(__ldg(base + off * hs)); };
-      gr[q][dir] = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, a.dc, dir);
+      gr[q][dir] = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, d0c<R>(a.dc, dir));
     }
   R M[22];
 #pragma unroll
@@ -197,7 +205,7 @@ __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int 
         if (per) l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
         return __ldg(E + (long long)(l2 - l) * st);
       };
-      s[d] = d0<R>(at, l, nn, per, cd8, a.dc, d);
+      s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
     }
     du[m + 1] = du[m + 1] + (s[0] + s[1] + s[2]) * ajac;
   }

@@ -87,6 +87,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_gpu_show_flow_msg.restype = C.c_int
     L.ocfd_gpu_ana_box.argtypes = [H, dp]
     L.ocfd_gpu_ana_box.restype = C.c_int
+    L.ocfd_gpu_profile_steps.argtypes = [H, C.c_int, dp]
+    L.ocfd_gpu_profile_steps.restype = C.c_int
     L.ocfd_batch_create.argtypes = [C.POINTER(H), C.c_int, C.POINTER(H)]
     L.ocfd_batch_create.restype = C.c_int
     L.ocfd_batch_step.argtypes = [H, C.c_int, C.c_int]
@@ -99,6 +101,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
 def lib(strict: bool = False) -> C.CDLL:
     """Load libocfdgpu.so (or the no-FMA strict build).  Raises if it is not built."""
     path = LIB_STRICT if strict else LIB_FAST
+    if not strict and os.environ.get("OCFD_GPU_LIB"):
+        path = os.environ["OCFD_GPU_LIB"]  # an alternative build of the same ABI
     if path not in _libs:
         if not os.path.exists(path):
             raise OSError(f"{path} is not built; run `make -C opencfd-sc_b200` (no CPU fallback exists)")
@@ -114,5 +118,5 @@ EXPORTED = [
     "ocfd_gpu_halo_prims", "ocfd_gpu_rhybrid", "ocfd_gpu_du_inviscous", "ocfd_gpu_du_inviscous_character",
     "ocfd_gpu_du_viscous", "ocfd_gpu_rk3", "ocfd_gpu_duvwt", "ocfd_gpu_bc", "ocfd_gpu_filter",
     "ocfd_gpu_advance_clock", "ocfd_gpu_step", "ocfd_gpu_show_flow_msg", "ocfd_gpu_ana_box", "ocfd_batch_create",
-    "ocfd_batch_step", "ocfd_batch_destroy",
+    "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps",
 ]

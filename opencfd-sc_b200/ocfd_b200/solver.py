@@ -206,6 +206,14 @@ class Solver:
         """n time steps on the fused, graph-captured path."""
         self._check(self.L.ocfd_gpu_step(self.h, n, 1 if sync else 0), "step")
 
+    PROFILE_GROUPS = ["sensor", "face_x", "face_y", "face_z", "visc_grad", "stage_tail", "negt_bc_halo", "step"]
+
+    def profile_steps(self, n: int = 3) -> dict:
+        """n eager steps with CUDA events around each kernel group (ms per step)."""
+        ms = np.zeros(8)
+        self._check(self.L.ocfd_gpu_profile_steps(self.h, n, _dp(ms)), "profile_steps")
+        return dict(zip(self.PROFILE_GROUPS, ms.tolist()))
+
     # ------------------------------------------------------------------ diagnostics
     def show_flow_msg(self) -> np.ndarray:
         e = np.zeros(3)

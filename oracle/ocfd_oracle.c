@@ -13,6 +13,7 @@
 #include "ocfd_oracle.h"
 
 #include <math.h>
+#include <omp.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -21,6 +22,13 @@
 #define DEL_NONE 0
 #define DEL_LIFT 1
 #define DEL_RIGHT 2
+
+struct pwork {
+  double *pc, *pd, *pu, *pv, *pw, *pa1, *pa2, *pa3;
+  double *pfp[5], *pfm[5];
+  double *ph1, *ph2, *phh[5];
+  int* scm;
+};
 
 struct ocfd_oracle {
   ocfd_params p;
@@ -33,12 +41,9 @@ struct ocfd_oracle {
   double *cc;
   double *ev[3];  /* Ev1..Ev3, each 4 haloed arrays */
   double *g[12];  /* uk ui us vk vi vs wk wi ws Tk Ti Ts (interior) */
-  /* pencil work arrays (OCFD_inviscous.f90:6-12) */
-  int npen;
-  double *pc, *pd, *pu, *pv, *pw, *pa1, *pa2, *pa3;
-  double *pfp[5], *pfm[5];
-  double *ph1, *ph2, *phh[5];
-  int* scm;
+  /* pencil work arrays (OCFD_inviscous.f90:6-12), one set per OpenMP thread */
+  int npen, nthreads;
+  struct pwork* pw;
   int istep;
   double tt;
 };
@@ -545,14 +550,19 @@ ocfd_oracle* orc_create(const ocfd_params* p) {
   for (int m = 0; m < 12; m++) o->g[m] = alloc_fill(o->n, 0.0);
   int nmax = o->nx; if (o->ny > nmax) nmax = o->ny; if (o->nz > nmax) nmax = o->nz;
   o->npen = nmax;
+  o->nthreads = omp_get_max_threads();
+  o->pw = (struct pwork*)calloc(o->nthreads, sizeof(struct pwork));
   size_t pl = (size_t)nmax + 2 * LAP;
-  double** pens[8] = {&o->pc, &o->pd, &o->pu, &o->pv, &o->pw, &o->pa1, &o->pa2, &o->pa3};
-  for (int m = 0; m < 8; m++) *pens[m] = alloc_fill(pl, 0.0);
-  for (int m = 0; m < 5; m++) { o->pfp[m] = alloc_fill(pl, 0.0); o->pfm[m] = alloc_fill(pl, 0.0); }
-  o->ph1 = alloc_fill(nmax + 1, 0.0);
-  o->ph2 = alloc_fill(nmax + 1, 0.0);
-  for (int m = 0; m < 5; m++) o->phh[m] = alloc_fill(nmax + 1, 0.0);
-  o->scm = (int*)calloc(nmax + 1, sizeof(int));
+  for (int t = 0; t < o->nthreads; t++) {
+    struct pwork* w = &o->pw[t];
+    double** pens[8] = {&w->pc, &w->pd, &w->pu, &w->pv, &w->pw, &w->pa1, &w->pa2, &w->pa3};
+    for (int m = 0; m < 8; m++) *pens[m] = alloc_fill(pl, 0.0);
+    for (int m = 0; m < 5; m++) { w->pfp[m] = alloc_fill(pl, 0.0); w->pfm[m] = alloc_fill(pl, 0.0); }
+    w->ph1 = alloc_fill(nmax + 1, 0.0);
+    w->ph2 = alloc_fill(nmax + 1, 0.0);
+    for (int m = 0; m < 5; m++) w->phh[m] = alloc_fill(nmax + 1, 0.0);
+    w->scm = (int*)calloc(nmax + 1, sizeof(int));
+  }
   return o;
 }
 
@@ -564,9 +574,13 @@ void orc_destroy(ocfd_oracle* o) {
   free(o->rhybrid); free(o->cc);
   for (int m = 0; m < 3; m++) free(o->ev[m]);
   for (int m = 0; m < 12; m++) free(o->g[m]);
-  free(o->pc); free(o->pd); free(o->pu); free(o->pv); free(o->pw); free(o->pa1); free(o->pa2); free(o->pa3);
-  for (int m = 0; m < 5; m++) { free(o->pfp[m]); free(o->pfm[m]); free(o->phh[m]); }
-  free(o->ph1); free(o->ph2); free(o->scm);
+  for (int t = 0; t < o->nthreads; t++) {
+    struct pwork* w = &o->pw[t];
+    free(w->pc); free(w->pd); free(w->pu); free(w->pv); free(w->pw); free(w->pa1); free(w->pa2); free(w->pa3);
+    for (int m = 0; m < 5; m++) { free(w->pfp[m]); free(w->pfm[m]); free(w->phh[m]); }
+    free(w->ph1); free(w->ph2); free(w->scm);
+  }
+  free(o->pw);
   free(o);
 }
 
@@ -645,6 +659,7 @@ void orc_d0(ocfd_oracle* o, int dir, const double* f, double* fx) {
   int nn = dir == 0 ? o->nx : (dir == 1 ? o->ny : o->nz);
   /* stride of the derivative direction in the haloed array */
   ptrdiff_t s = dir == 0 ? 1 : (dir == 1 ? (ptrdiff_t)o->nxh : (ptrdiff_t)o->nxh * o->nyh);
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= o->nz; k++)
     for (int j = 1; j <= o->ny; j++)
       for (int i = 1; i <= o->nx; i++) {
@@ -1122,19 +1137,17 @@ static void hybrid_index(ocfd_oracle* o, int dir, int a, int b, int nn, int* scm
   }
 }
 
-static void pencil_ptrs(ocfd_oracle* o, double** pen, double** fp, double** fm) {
-  double* base[8] = {o->pc, o->pd, o->pu, o->pv, o->pw, o->pa1, o->pa2, o->pa3};
+static void pencil_ptrs(struct pwork* w, double** pen, double** fp, double** fm) {
+  double* base[8] = {w->pc, w->pd, w->pu, w->pv, w->pw, w->pa1, w->pa2, w->pa3};
   for (int q = 0; q < 8; q++) pen[q] = base[q] + LAP - 1;
-  for (int m = 0; m < 5; m++) { fp[m] = o->pfp[m] + LAP - 1; fm[m] = o->pfm[m] + LAP - 1; }
+  for (int m = 0; m < 5; m++) { fp[m] = w->pfp[m] + LAP - 1; fm[m] = w->pfm[m] + LAP - 1; }
 }
 
-/* du_inviscous: OCFD_inviscous.f90:53-203 */
+/* du_inviscous: OCFD_inviscous.f90:53-203.  Pencils are independent: OpenMP
+ * over the pencils of one direction (the directions stay in order). */
 void orc_du_inviscous(ocfd_oracle* o) {
   const ocfd_params* p = &o->p;
   double hx_1 = 1.0 / p->hx, hy_1 = 1.0 / p->hy, hz_1 = 1.0 / p->hz;
-  double* pen[8];
-  double *fp[5], *fm[5];
-  pencil_ptrs(o, pen, fp, fm);
   compute_cc(o);
   int nx = o->nx, ny = o->ny, nz = o->nz;
   for (int dir = 0; dir < 3; dir++) {
@@ -1143,27 +1156,33 @@ void orc_du_inviscous(ocfd_oracle* o) {
     const int* bi = p->bound_index + 2 * dir;
     const int* sb = p->scheme_boundary + 2 * dir;
     double h_1 = dir == 0 ? hx_1 : (dir == 1 ? hy_1 : hz_1);
-    for (int b = 1; b <= nb; b++)
+#pragma omp parallel for schedule(static)
+    for (int b = 1; b <= nb; b++) {
+      struct pwork* w = &o->pw[omp_get_thread_num()];
+      double* pen[8];
+      double *fp[5], *fm[5];
+      pencil_ptrs(w, pen, fp, fm);
       for (int a = 1; a <= na; a++) {
-        if (p->scheme_invis == OCFD_SCHEME_HYBRID) hybrid_index(o, dir, a, b, nn, o->scm);
-        else memset(o->scm, 0, sizeof(int) * (nn + 1));
+        if (p->scheme_invis == OCFD_SCHEME_HYBRID) hybrid_index(o, dir, a, b, nn, w->scm);
+        else memset(w->scm, 0, sizeof(int) * (nn + 1));
         gather_pencil(o, dir, a, b, pen);
         if (p->flux_splitting == OCFD_SPLIT_SW) split_sw(p, nn, pen[0], pen[1], pen[2], pen[3], pen[4], pen[5], pen[6], pen[7], fp, fm);
         else split_llf(p, nn, pen[0], pen[1], pen[2], pen[3], pen[4], pen[5], pen[6], pen[7], fp, fm);
         for (int m = 1; m <= 5; m++) {
-          ocfd2d_flux1(p, fp[m - 1], o->ph1, nn, bi, o->scm, sb);
-          ocfd2d_flux2(p, fm[m - 1], o->ph2, nn, bi, o->scm, sb);
+          ocfd2d_flux1(p, fp[m - 1], w->ph1, nn, bi, w->scm, sb);
+          ocfd2d_flux2(p, fm[m - 1], w->ph2, nn, bi, w->scm, sb);
           for (int l = 1; l <= nn; l++) {
             int i, j, k;
             if (dir == 0) { i = l; j = a; k = b; } else if (dir == 1) { i = a; j = l; k = b; } else { i = a; j = b; k = l; }
             size_t c = IF(o, i, j, k, m);
-            double dd = (o->ph1[l] - o->ph1[l - 1] + o->ph2[l] - o->ph2[l - 1]) * h_1;
+            double dd = (w->ph1[l] - w->ph1[l - 1] + w->ph2[l] - w->ph2[l - 1]) * h_1;
             if (dir == 0) o->du[c] = dd;
             else if (dir == 1) o->du[c] = o->du[c] + dd;
             else o->du[c] = -(o->du[c] + dd) * o->met[OCFD_M_AJAC][IH(o, i, j, k)];
           }
         }
       }
+    }
   }
   if (p->if_mass_force == 1) {
     /* OCFD_inviscous.f90:189-201 */
@@ -1277,7 +1296,7 @@ static void flux_charteric(ocfd_oracle* o, int nn, double** hh, double** fp, dou
   const double *cc = pen[0], *uu = pen[2], *vv = pen[3], *ww = pen[4];
   const double *AA1 = pen[5], *AA2 = pen[6], *AA3 = pen[7];
   /* fpc(Ka1:Kb1,5), fmc(Ka2:Kb2,5) persist across faces, as in the reference */
-  static double fpc_s[5][16], fmc_s[5][16];
+  double fpc_s[5][16] = {{0}}, fmc_s[5][16] = {{0}};
   double S[25] = {0}, S1[25] = {0};
   int ia = (bi[0] == 0 || sb[0] != 0) ? 0 : 1;
   int ib = (bi[1] == 0 || sb[1] != 0) ? nn : nn - 1;
@@ -1343,9 +1362,6 @@ static void flux_charteric(ocfd_oracle* o, int nn, double** hh, double** fp, dou
 void orc_du_inviscous_character(ocfd_oracle* o) {
   const ocfd_params* p = &o->p;
   double hx_1 = 1.0 / p->hx, hy_1 = 1.0 / p->hy, hz_1 = 1.0 / p->hz;
-  double* pen[8];
-  double *fp[5], *fm[5];
-  pencil_ptrs(o, pen, fp, fm);
   compute_cc(o);
   int nx = o->nx, ny = o->ny, nz = o->nz;
   for (int dir = 0; dir < 3; dir++) {
@@ -1354,25 +1370,31 @@ void orc_du_inviscous_character(ocfd_oracle* o) {
     const int* bi = p->bound_index + 2 * dir;
     const int* sb = p->scheme_boundary + 2 * dir;
     double h_1 = dir == 0 ? hx_1 : (dir == 1 ? hy_1 : hz_1);
-    for (int b = 1; b <= nb; b++)
+#pragma omp parallel for schedule(static)
+    for (int b = 1; b <= nb; b++) {
+      struct pwork* w = &o->pw[omp_get_thread_num()];
+      double* pen[8];
+      double *fp[5], *fm[5];
+      pencil_ptrs(w, pen, fp, fm);
       for (int a = 1; a <= na; a++) {
-        if (p->scheme_invis == OCFD_SCHEME_HYBRID) hybrid_index(o, dir, a, b, nn, o->scm);
-        else memset(o->scm, 0, sizeof(int) * (nn + 1));
+        if (p->scheme_invis == OCFD_SCHEME_HYBRID) hybrid_index(o, dir, a, b, nn, w->scm);
+        else memset(w->scm, 0, sizeof(int) * (nn + 1));
         gather_pencil(o, dir, a, b, pen);
         if (p->flux_splitting == OCFD_SPLIT_SW) split_sw(p, nn, pen[0], pen[1], pen[2], pen[3], pen[4], pen[5], pen[6], pen[7], fp, fm);
         else split_llf(p, nn, pen[0], pen[1], pen[2], pen[3], pen[4], pen[5], pen[6], pen[7], fp, fm);
-        flux_charteric(o, nn, o->phh, fp, fm, pen, bi, o->scm, sb);
+        flux_charteric(o, nn, w->phh, fp, fm, pen, bi, w->scm, sb);
         for (int m = 1; m <= 5; m++)
           for (int l = 1; l <= nn; l++) {
             int i, j, k;
             if (dir == 0) { i = l; j = a; k = b; } else if (dir == 1) { i = a; j = l; k = b; } else { i = a; j = b; k = l; }
             size_t c = IF(o, i, j, k, m);
-            double dd = (o->phh[m - 1][l] - o->phh[m - 1][l - 1]) * h_1;
+            double dd = (w->phh[m - 1][l] - w->phh[m - 1][l - 1]) * h_1;
             if (dir == 0) o->du[c] = dd;
             else if (dir == 1) o->du[c] = o->du[c] + dd;
             else o->du[c] = -(o->du[c] + dd) * o->met[OCFD_M_AJAC][IH(o, i, j, k)];
           }
       }
+    }
   }
   if (p->if_mass_force == 1) {
     for (int k = 1; k <= nz; k++)
@@ -1420,6 +1442,7 @@ void orc_du_viscous(ocfd_oracle* o) {
   orc_d0(o, 0, o->u, g[0]); orc_d0(o, 0, o->v, g[3]); orc_d0(o, 0, o->w, g[6]); orc_d0(o, 0, o->T, g[9]);
   orc_d0(o, 1, o->u, g[1]); orc_d0(o, 1, o->v, g[4]); orc_d0(o, 1, o->w, g[7]); orc_d0(o, 1, o->T, g[10]);
   orc_d0(o, 2, o->u, g[2]); orc_d0(o, 2, o->v, g[5]); orc_d0(o, 2, o->w, g[8]); orc_d0(o, 2, o->T, g[11]);
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= o->nz; k++)
     for (int j = 1; j <= o->ny; j++)
       for (int i = 1; i <= o->nx; i++) {
@@ -1474,6 +1497,7 @@ void orc_du_viscous(ocfd_oracle* o) {
     orc_d0(o, 0, E1, g[0]);
     orc_d0(o, 1, E2, g[1]);
     orc_d0(o, 2, E3, g[2]);
+#pragma omp parallel for schedule(static)
     for (int k = 1; k <= o->nz; k++)
       for (int j = 1; j <= o->ny; j++)
         for (int i = 1; i <= o->nx; i++) {
@@ -1491,9 +1515,11 @@ void orc_rk3(ocfd_oracle* o, int krk) {
   double dt = o->p.dt;
   size_t n5 = 5 * o->n;
   if (krk == 1) {
+#pragma omp parallel for schedule(static)
     for (size_t c = 0; c < n5; c++) o->f[c] = o->fn[c] + dt * o->du[c];
   } else {
     double a = Ralfa[krk - 1], b = Rbeta[krk - 1];
+#pragma omp parallel for schedule(static)
     for (size_t c = 0; c < n5; c++) o->f[c] = a * o->fn[c] + b * (o->f[c] + dt * o->du[c]);
   }
 }

@@ -103,24 +103,34 @@ def hit_coords(n: int):
 def hit_prims(n: int, mt: float, ma: float, k0: float = 4.0, seed: int = 20261203):
     """Seeded solenoidal random-phase velocity with E(k) ~ k^4 exp(-2 (k/k0)^2),
     scaled to turbulent Mach number mt = sqrt(<u^2+v^2+w^2>)/<c> with c = sqrt(T)/Ma
-    (the ana_box definitions, OCFD_ANA.f90:227,265); rho = T = 1."""
+    (the ana_box definitions, OCFD_ANA.f90:227,265); rho = T = 1.  Built on the
+    real-to-complex half spectrum with broadcast wavenumbers, so the host memory
+    peak stays near 8 GB at 512^3."""
     rng = np.random.default_rng(seed)
     k = np.fft.fftfreq(n, d=1.0 / n)
-    KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
-    kk = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
-    kk[0, 0, 0] = 1.0
-    amp = np.sqrt(kk ** 4 * np.exp(-2.0 * (kk / k0) ** 2) / (4.0 * np.pi * kk ** 2))
+    kr = np.fft.rfftfreq(n, d=1.0 / n)
+    KZ = k[:, None, None]
+    KY = k[None, :, None]
+    KX = kr[None, None, :]
+    kk2 = KZ ** 2 + KY ** 2 + KX ** 2
+    kk2[0, 0, 0] = 1.0
+    kk = np.sqrt(kk2)
+    amp = np.sqrt(kk ** 4 * np.exp(-2.0 * (kk / k0) ** 2) / (4.0 * np.pi * kk2))
     amp[0, 0, 0] = 0.0
-    comps = []
-    for _ in range(3):
-        ph = rng.uniform(0, 2 * np.pi, size=kk.shape)
-        comps.append(amp * np.exp(1j * ph))
-    # solenoidal projection
-    dot = (comps[0] * KX + comps[1] * KY + comps[2] * KZ) / (kk ** 2)
-    comps = [comps[0] - dot * KX, comps[1] - dot * KY, comps[2] - dot * KZ]
-    vel = [np.real(np.fft.ifftn(c)) for c in comps]
+    del kk
+    comps = [amp * np.exp(1j * rng.uniform(0, 2 * np.pi, size=amp.shape)) for _ in range(3)]
+    del amp
+    # solenoidal projection: c -= (c.k) k / |k|^2
+    dot = (comps[0] * KX + comps[1] * KY + comps[2] * KZ) / kk2
+    comps[0] -= dot * KX
+    comps[1] -= dot * KY
+    comps[2] -= dot * KZ
+    del dot, kk2
+    vel = []
+    while comps:
+        vel.append(np.fft.irfftn(comps.pop(0), s=(n, n, n)))
     c_mean = 1.0 / ma
-    rms = math.sqrt(float(np.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)))
+    rms = math.sqrt(float(np.mean(vel[0] ** 2) + np.mean(vel[1] ** 2) + np.mean(vel[2] ** 2)))
     s = mt * c_mean / rms
     u, v, w = [np.ascontiguousarray(a * s) for a in vel]
     d = np.ones_like(u)

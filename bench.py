@@ -265,7 +265,8 @@ def run_ours(args):
     t_launch = groups[dom] / 3.0 * 1e-3  # 3 launches per step
     achieved = model[dom] * n / t_launch / 1e9
     peak, peak_kind = load_peaks()
-    traffic = load_traffic().get(f"{args.workload}:{args.precision}:{dom}")
+    bpp = load_traffic().get(f"{args.workload}:{args.precision}:{dom}")
+    traffic = None if bpp is None else bpp * n  # DRAM bytes per launch, scaled from a 128^3 capture
 
     # ---- end to end through the C ABI with host-owned state: per step, upload
     # f + haloed primitives from pinned host memory, one time step, download them.

@@ -266,6 +266,28 @@ int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]);
  * d_rms, T_aver, Amu_aver, d_aver, Ux_rms, Alamdax. */
 int ocfd_gpu_ana_box(ocfd_handle* h, double out[20]);
 
+/* show_flow_msg on arrays the caller owns, allocating nothing.  No counterpart
+ * in the reference: it is for callers that cannot allocate device memory (a
+ * host solver whose device memory all belongs to its own pool, or code that
+ * must not trigger cudaFree's device-wide synchronisation while other streams
+ * run), so they cannot create an ocfd_handle.
+ *   p      parameters after ocfd_set_parameters (nx, ny, nz, gamma, Ma are read)
+ *   f      device (nx,ny,nz,5) conserved variables, Fortran order
+ *   prims  device haloed d, u, v, w, T ((nx+8)(ny+8)(nz+8) each, LAP = 4)
+ *   ajac   device haloed Jacobian, same layout
+ *   stream cudaStream_t (NULL: the default stream); the call waits for it
+ * E0 receives the same three averages as ocfd_gpu_show_flow_msg (equal within
+ * rounding: the summation order differs).  The partial sums live in a fixed
+ * static device array of OCFD_NOALLOC_MAX_PLANES k-planes: nz above that is
+ * rejected with OCFD_E_PARAM.  Nothing in that array has to start at zero.
+ * The first call on a device, made with that device current, looks up the
+ * array's address (once per device); make that first call before any stream
+ * capture begins.  There is one array per device, so overlapping calls on the
+ * same device (from several streams or host threads) race: serialise them. */
+#define OCFD_NOALLOC_MAX_PLANES 4096
+int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f, const double* const prims[5],
+                               const double* ajac, void* stream, double E0[3]);
+
 /* ---------------------------------------------------------------------------
  * Ensemble (batched) mode: several independent instances advanced together,
  * one fused launch per kernel and per RK stage for all of them, captured as

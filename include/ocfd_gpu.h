@@ -289,16 +289,31 @@ int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f, const doub
                                const double* ajac, void* stream, double E0[3]);
 
 /* ---------------------------------------------------------------------------
- * Ensemble (batched) mode: several independent instances advanced together,
- * one fused launch per kernel and per RK stage for all of them, captured as
- * one CUDA graph.  The instances keep their own state and parameters; they
- * must share the scheme configuration (schemes, splitting, character flag,
- * boundary configuration, precision).  Replaces nothing in the reference
- * (which runs one case per process); used by the serving loop.
+ * Ensemble (batched) mode: several independent instances advanced together.
+ * No counterpart in the reference (which runs one case per process); used by
+ * the serving loop.  Members keep their own state, grid size and physical
+ * parameters (Re, Ma, dt, splitting).  When all members are periodic in the
+ * three directions (BC_None, no ghost cells, no filter) and share precision,
+ * flux form, inviscid scheme and the viscous flag, a time step is one launch
+ * per kernel and per RK stage for the whole batch (18 launches, ragged grids
+ * in the same launch), captured as a CUDA graph; the face-sweep tile shape per
+ * direction is chosen by timing the candidates on the first step
+ * (autotuning).  Otherwise the members advance concurrently on their own
+ * streams.  Results are bit-identical to stepping each member alone.
+ * Between batch steps a member may be used on its own (downloads,
+ * diagnostics, single steps); the batch rebuilds its tables when needed.
  * ------------------------------------------------------------------------- */
 typedef struct ocfd_batch ocfd_batch;
 int ocfd_batch_create(ocfd_handle* const* members, int count, ocfd_batch** out);
+/* nsteps time steps of every member; sync = 1 waits and checks every member's
+ * negative-temperature status (OCFD_E_NEGT if any member exceeded the limit). */
 int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync);
+/* Force the face tile variant per direction (0 or 1; -1 = autotune). */
+int ocfd_batch_set_tiles(ocfd_batch* b, const int variants[3]);
+/* *fused = 1 when the batch runs one launch per kernel for all members;
+ * variants[3] = the tile variants in use (after the first step). */
+int ocfd_batch_info(const ocfd_batch* b, int* fused, int variants[3]);
+const char* ocfd_batch_last_error(const ocfd_batch* b);
 void ocfd_batch_destroy(ocfd_batch* b);
 
 #ifdef __cplusplus

@@ -565,40 +565,45 @@ int ocfd_gpu_rhybrid(ocfd_handle* h) {
 
 }  // extern "C"
 
+template <typename S>
+static FaceArgs<S> face_args(ocfd_handle* h, int d) {
+  const Grid& g = h->g;
+  FaceArgs<S> a;
+  a.g = g;
+  a.ph = h->ph;
+  if (std::is_same<S, float>::value) {
+    a.d = (const S*)h->p32[0];
+    a.u = (const S*)h->p32[1];
+    a.v = (const S*)h->p32[2];
+    a.w = (const S*)h->p32[3];
+    a.T = (const S*)h->p32[4];
+    a.A1 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d];
+    a.A2 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 1];
+    a.A3 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 2];
+  } else {
+    a.d = (const S*)h->prim[0];
+    a.u = (const S*)h->prim[1];
+    a.v = (const S*)h->prim[2];
+    a.w = (const S*)h->prim[3];
+    a.T = (const S*)h->prim[4];
+    a.A1 = (const S*)h->met[OCFD_M_AKX1 + 3 * d];
+    a.A2 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 1];
+    a.A3 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 2];
+  }
+  a.rh = h->rh;
+  a.hh = h->hf[d];
+  a.fs = h->fs[d];
+  a.fbeg = h->ph.periodic[d] ? 1 : 0;
+  a.fend = g.len(d);
+  a.split = h->p.flux_splitting;
+  return a;
+}
+
 template <typename R, typename S>
 static int faces(ocfd_handle* h, int dsel = -1) {
-  const Grid& g = h->g;
   for (int d = 0; d < 3; d++) {
     if (dsel >= 0 && d != dsel) continue;
-    FaceArgs<S> a;
-    a.g = g;
-    a.ph = h->ph;
-    if (std::is_same<S, float>::value) {
-      a.d = (const S*)h->p32[0];
-      a.u = (const S*)h->p32[1];
-      a.v = (const S*)h->p32[2];
-      a.w = (const S*)h->p32[3];
-      a.T = (const S*)h->p32[4];
-      a.A1 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d];
-      a.A2 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 1];
-      a.A3 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 2];
-    } else {
-      a.d = (const S*)h->prim[0];
-      a.u = (const S*)h->prim[1];
-      a.v = (const S*)h->prim[2];
-      a.w = (const S*)h->prim[3];
-      a.T = (const S*)h->prim[4];
-      a.A1 = (const S*)h->met[OCFD_M_AKX1 + 3 * d];
-      a.A2 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 1];
-      a.A3 = (const S*)h->met[OCFD_M_AKX1 + 3 * d + 2];
-    }
-    a.rh = h->rh;
-    a.hh = h->hf[d];
-    a.fs = h->fs[d];
-    a.fbeg = h->ph.periodic[d] ? 1 : 0;
-    a.fend = g.len(d);
-    a.split = h->p.flux_splitting;
-    CK((launch_face<R, S>(d, h->chr, h->p.scheme_invis, a, h->st)));
+    CK((launch_face<R, S>(d, h->chr, h->p.scheme_invis, face_args<S>(h, d), h->st)));
   }
   return OCFD_OK;
 }
@@ -666,7 +671,7 @@ int ocfd_gpu_du_inviscous_character(ocfd_handle* h) {
 }  // extern "C"
 
 template <typename R, typename S>
-static int visc_grad(ocfd_handle* h) {
+static ViscArgs<R, S> visc_args(ocfd_handle* h) {
   ViscArgs<R, S> a;
   a.g = h->g;
   a.ph = h->ph;
@@ -687,7 +692,12 @@ static int visc_grad(ocfd_handle* h) {
     for (int m = 0; m < 22; m++) a.met[m] = (const S*)h->met[m];
   }
   a.ev = (R*)h->ev;
-  CK((launch_visc_grad<R, S>(a, h->st)));
+  return a;
+}
+
+template <typename R, typename S>
+static int visc_grad(ocfd_handle* h) {
+  CK((launch_visc_grad<R, S>(visc_args<R, S>(h), h->st)));
   return OCFD_OK;
 }
 
@@ -985,36 +995,455 @@ int ocfd_gpu_ana_box(ocfd_handle* h, double out[20]) {
   return OCFD_OK;
 }
 
+}  // extern "C"
+
 // ------------------------------------------------------------------ batch (ensemble)
+// Several instances advanced together.  When every member is periodic in all
+// three directions with the fused boundary path, shares precision, flux form,
+// inviscid scheme and viscous flag, and filters nothing, a time step is
+// 3 stages x (3 face sweeps + viscous gradients + stage tail + negative-T
+// repair) = 18 launches for the whole batch, whatever its size: each launch
+// covers the blocks of every member (ragged grids), and a table in device
+// memory gives each block its member's arguments.  The step is captured as one
+// CUDA graph per buffer parity (the (f, fn) and temperature buffers of every
+// member swap once per step, so two graphs alternate).  Otherwise the members
+// advance concurrently on their own streams from their own graphs.
 struct ocfd_batch {
   std::vector<ocfd_handle*> m;
+  int device = 0;
   cudaStream_t st = nullptr;
-  std::vector<cudaEvent_t> ev;
+  std::vector<cudaEvent_t> ev;  // one per member (member -> batch ordering)
+  cudaEvent_t done = nullptr;   // batch -> members
+  bool fused = false;
+  int variant[3] = {0, 0, 0};   // face tile variant per direction
+  int forced[3] = {-1, -1, -1};
+  bool tuned = false;
+  // per parity: device tables and the captured step
+  struct Par {
+    void* dev = nullptr;
+    size_t bytes = 0;
+    cudaGraphExec_t graph = nullptr;
+  } par[2];
+  std::vector<double*> f0, t0;  // members' f and T at table build (parity 0)
+  int nblk_face[3] = {0, 0, 0}, nblk_upd = 0;
+  std::string err;
 };
+
+namespace {
+
+int bfail(ocfd_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+#define BCK(call)                                                                   \
+  do {                                                                              \
+    cudaError_t e__ = (call);                                                       \
+    if (e__ != cudaSuccess) return bfail(b, OCFD_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+bool batch_fusable(const std::vector<ocfd_handle*>& m) {
+  const ocfd_handle* a = m[0];
+  for (const ocfd_handle* h : m) {
+    if (h->device != a->device || !h->fuse_bc || h->p.nfiltering != 0) return false;
+    for (int d = 0; d < 3; d++)
+      if (!h->ph.periodic[d]) return false;
+    if (h->mixed != a->mixed || h->chr != a->chr || h->p.scheme_invis != a->p.scheme_invis ||
+        (h->p.if_viscous != 0) != (a->p.if_viscous != 0))
+      return false;
+  }
+  return true;
+}
+
+// Host image of one parity's tables: per stage, per direction the face
+// arguments; per stage the viscous, tail and repair arguments; the block
+// ranges (int4) shared by all stages.
+struct Image {
+  std::vector<unsigned char> buf;
+  size_t put(const void* src, size_t n) {
+    size_t off = (buf.size() + 255) & ~size_t(255);
+    buf.resize(off + n);
+    memcpy(buf.data() + off, src, n);
+    return off;
+  }
+};
+
+template <typename R>
+struct StageOffsets {
+  size_t face[3], visc, upd, negt;
+};
+
+void block_ranges(const std::vector<dim3>& dims, std::vector<int4>& ent, int& total) {
+  ent.resize(dims.size());
+  long long start = 0;
+  for (size_t q = 0; q < dims.size(); q++) {
+    ent[q] = make_int4((int)start, (int)dims[q].x, (int)dims[q].y, 0);
+    start += (long long)dims[q].x * dims[q].y * dims[q].z;
+  }
+  total = (int)start;
+}
+
+}  // namespace
+
+// Builds the tables of one parity and captures its step graph.  The members'
+// buffer pointers are advanced through the step exactly as fused_step does and
+// restored afterwards.
+template <typename R>
+static int batch_capture(ocfd_batch* b, int parity) {
+  typedef R S;
+  std::vector<ocfd_handle*>& M = b->m;
+  const int n = (int)M.size();
+  const ocfd_handle* h0 = M[0];
+  struct Saved {
+    double *f, *fn, *t, *ta;
+  };
+  std::vector<Saved> sv(n);
+  for (int q = 0; q < n; q++) sv[q] = {M[q]->f, M[q]->fn, M[q]->prim[4], M[q]->talt};
+  auto restore = [&]() {
+    for (int q = 0; q < n; q++) {
+      M[q]->f = sv[q].f;
+      M[q]->fn = sv[q].fn;
+      M[q]->prim[4] = sv[q].t;
+      M[q]->talt = sv[q].ta;
+    }
+  };
+  if (parity == 1)
+    for (ocfd_handle* h : M) {
+      std::swap(h->f, h->fn);
+      std::swap(h->prim[4], h->talt);
+    }
+  // block ranges (independent of the stage)
+  std::vector<int4> ent_face[3], ent_upd;
+  for (int d = 0; d < 3; d++) {
+    std::vector<dim3> dims(n);
+    for (int q = 0; q < n; q++) dims[q] = face_batch_dims<S>(d, b->variant[d], face_args<S>(M[q], d));
+    block_ranges(dims, ent_face[d], b->nblk_face[d]);
+  }
+  {
+    std::vector<dim3> dims(n);
+    for (int q = 0; q < n; q++) dims[q] = update_dims(M[q]->g);
+    block_ranges(dims, ent_upd, b->nblk_upd);
+  }
+  Image im;
+  size_t o_ent_face[3], o_ent_upd;
+  for (int d = 0; d < 3; d++) o_ent_face[d] = im.put(ent_face[d].data(), n * sizeof(int4));
+  o_ent_upd = im.put(ent_upd.data(), n * sizeof(int4));
+  StageOffsets<R> so[3];
+  for (ocfd_handle* h : M) std::swap(h->f, h->fn);  // fn = f (fused_step)
+  for (int krk = 1; krk <= 3; krk++) {
+    StageOffsets<R>& o = so[krk - 1];
+    for (int d = 0; d < 3; d++) {
+      std::vector<FaceArgs<S>> fa(n);
+      for (int q = 0; q < n; q++) fa[q] = face_args<S>(M[q], d);
+      o.face[d] = im.put(fa.data(), n * sizeof(FaceArgs<S>));
+    }
+    std::vector<ViscArgs<R, S>> va(n);
+    for (int q = 0; q < n; q++) va[q] = visc_args<R, S>(M[q]);
+    o.visc = im.put(va.data(), n * sizeof(ViscArgs<R, S>));
+    std::vector<UpdArgs<R>> ua(n);
+    std::vector<UpdArgs<double>> na(n);
+    for (int q = 0; q < n; q++) {
+      ua[q] = upd_args<R>(M[q]);
+      ua[q].krk = krk;
+      ua[q].du = nullptr;
+      na[q] = upd_args<double>(M[q]);
+    }
+    o.upd = im.put(ua.data(), n * sizeof(UpdArgs<R>));
+    o.negt = im.put(na.data(), n * sizeof(UpdArgs<double>));
+    for (ocfd_handle* h : M) swap_t(h);
+  }
+  restore();
+  // upload
+  ocfd_batch::Par& P = b->par[parity];
+  if (P.graph) {
+    cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+  }
+  if (P.bytes < im.buf.size()) {
+    if (P.dev) cudaFree(P.dev);
+    P.dev = nullptr;
+    BCK(cudaMalloc(&P.dev, im.buf.size()));
+    P.bytes = im.buf.size();
+  }
+  BCK(cudaMemcpy(P.dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice));
+  unsigned char* base = (unsigned char*)P.dev;
+  auto tab = [&](size_t args_off, size_t ent_off) {
+    struct {
+      const void* a;
+      const int4* e;
+    } t = {base + args_off, (const int4*)(base + ent_off)};
+    return t;
+  };
+  // capture: per stage the sensor (per member), 3 face sweeps, the viscous
+  // gradients, the tail and the repair, all on the batch stream
+  const bool hybrid = h0->p.scheme_invis == OCFD_SCHEME_HYBRID;
+  std::vector<cudaStream_t> own(n);
+  for (int q = 0; q < n; q++) own[q] = M[q]->st;
+  cudaGraph_t graph;
+  BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  int r = OCFD_OK;
+  cudaError_t e = cudaSuccess;
+  if (parity == 1)
+    for (ocfd_handle* h : M) {
+      std::swap(h->f, h->fn);
+      std::swap(h->prim[4], h->talt);
+    }
+  for (ocfd_handle* h : M) std::swap(h->f, h->fn);
+  for (int krk = 1; krk <= 3 && r == OCFD_OK && e == cudaSuccess; krk++) {
+    const StageOffsets<R>& o = so[krk - 1];
+    if (hybrid && krk == 1)
+      for (int q = 0; q < n && r == OCFD_OK; q++) {
+        M[q]->st = b->st;  // the sensor's launches join the capture
+        r = ocfd_gpu_rhybrid(M[q]);
+        M[q]->st = own[q];
+      }
+    for (int d = 0; d < 3 && e == cudaSuccess; d++) {
+      auto t = tab(o.face[d], o_ent_face[d]);
+      BatchTab<FaceArgs<S>> bt = {(const FaceArgs<S>*)t.a, t.e, n};
+      e = launch_face_batch<R, S>(d, h0->chr, h0->p.scheme_invis, b->variant[d], bt, b->nblk_face[d], b->st);
+    }
+    if (e == cudaSuccess && h0->p.if_viscous) {
+      auto t = tab(o.visc, o_ent_upd);
+      BatchTab<ViscArgs<R, S>> bt = {(const ViscArgs<R, S>*)t.a, t.e, n};
+      e = launch_visc_grad_batch<R, S>(bt, b->nblk_upd, b->st);
+    }
+    if (e == cudaSuccess) {
+      auto t = tab(o.upd, o_ent_upd);
+      BatchTab<UpdArgs<R>> bt = {(const UpdArgs<R>*)t.a, t.e, n};
+      e = launch_fused_batch<R>(bt, b->nblk_upd, h0->chr, h0->p.if_viscous != 0, true, b->st);
+    }
+    if (e == cudaSuccess) {
+      auto t = tab(o.negt, o_ent_upd);
+      BatchTab<UpdArgs<double>> bt = {(const UpdArgs<double>*)t.a, t.e, n};
+      e = launch_negt_fix_batch(bt, b->st);
+    }
+    for (ocfd_handle* h : M) swap_t(h);
+  }
+  cudaError_t ec = cudaStreamEndCapture(b->st, &graph);
+  restore();
+  if (r) return bfail(b, r, "sensor launch during capture: " + M[0]->err);
+  if (e != cudaSuccess) return bfail(b, OCFD_E_CUDA, std::string("batched launch: ") + cudaGetErrorString(e));
+  if (ec != cudaSuccess) return bfail(b, OCFD_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ec));
+  ec = cudaGraphInstantiate(&P.graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ec != cudaSuccess) return bfail(b, OCFD_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ec));
+  return OCFD_OK;
+}
+
+// Times each face tile variant per direction on the members' current state
+// (the face sweeps only write the face-flux buffers, which every stage
+// rewrites before reading) and keeps the faster one.
+template <typename R>
+static int batch_autotune(ocfd_batch* b) {
+  typedef R S;
+  std::vector<ocfd_handle*>& M = b->m;
+  const int n = (int)M.size();
+  const ocfd_handle* h0 = M[0];
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  void* dev = nullptr;
+  int rc = OCFD_OK;
+  for (int d = 0; d < 3 && rc == OCFD_OK; d++) {
+    if (b->forced[d] >= 0) {
+      b->variant[d] = b->forced[d];
+      continue;
+    }
+    float best = 1e30f;
+    for (int v = 0; v < 2 && rc == OCFD_OK; v++) {
+      std::vector<dim3> dims(n);
+      std::vector<FaceArgs<S>> fa(n);
+      for (int q = 0; q < n; q++) {
+        fa[q] = face_args<S>(M[q], d);
+        dims[q] = face_batch_dims<S>(d, v, fa[q]);
+      }
+      std::vector<int4> ent;
+      int nblk = 0;
+      block_ranges(dims, ent, nblk);
+      Image im;
+      const size_t oa = im.put(fa.data(), n * sizeof(FaceArgs<S>)), oe = im.put(ent.data(), n * sizeof(int4));
+      if (!dev && cudaMalloc(&dev, im.buf.size() + 4096) != cudaSuccess) {
+        rc = bfail(b, OCFD_E_NOMEM, "autotune table");
+        break;
+      }
+      cudaMemcpy(dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice);
+      BatchTab<FaceArgs<S>> bt = {(const FaceArgs<S>*)((unsigned char*)dev + oa),
+                                  (const int4*)((unsigned char*)dev + oe), n};
+      float tot = 0.f;
+      for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, b->st);
+        cudaError_t e = launch_face_batch<R, S>(d, h0->chr, h0->p.scheme_invis, v, bt, nblk, b->st);
+        cudaEventRecord(e1, b->st);
+        if (e != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = bfail(b, OCFD_E_CUDA, "autotune launch");
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) tot += ms;  // first launch is a warm-up
+      }
+      if (tot < best) {
+        best = tot;
+        b->variant[d] = v;
+      }
+      if (dev) {
+        cudaFree(dev);
+        dev = nullptr;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+static int batch_prepare(ocfd_batch* b) {
+  BCK(cudaStreamSynchronize(b->st));  // no launch in flight reads the old tables
+  for (int P = 0; P < 2; P++)
+    if (b->par[P].graph) {
+      cudaGraphExecDestroy(b->par[P].graph);
+      b->par[P].graph = nullptr;
+    }
+  const bool mixed = b->m[0]->mixed;
+  int r = OCFD_OK;
+  if (!b->tuned) {
+    r = mixed ? batch_autotune<float>(b) : batch_autotune<double>(b);
+    if (r) return r;
+    b->tuned = true;
+  }
+  for (int P = 0; P < 2 && r == OCFD_OK; P++) r = mixed ? batch_capture<float>(b, P) : batch_capture<double>(b, P);
+  if (r) return r;
+  b->f0.clear();
+  b->t0.clear();
+  for (ocfd_handle* h : b->m) {
+    b->f0.push_back(h->f);
+    b->t0.push_back(h->prim[4]);
+  }
+  return OCFD_OK;
+}
+
+extern "C" {
 
 int ocfd_batch_create(ocfd_handle* const* members, int count, ocfd_batch** out) {
   if (!members || count <= 0 || !out) return OCFD_E_PARAM;
+  *out = nullptr;
+  for (int q = 0; q < count; q++)
+    if (!members[q]) return OCFD_E_PARAM;
   ocfd_batch* b = new ocfd_batch();
   for (int q = 0; q < count; q++) b->m.push_back(members[q]);
+  b->device = members[0]->device;
+  b->fused = batch_fusable(b->m);
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+  for (int q = 0; q < count && e == cudaSuccess; q++) {
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) b->ev.push_back(ev);
+  }
+  if (e == cudaSuccess && b->fused) e = b->m[0]->mixed ? setup_face_batch_kernels_f32() : setup_face_batch_kernels_f64();
+  if (e != cudaSuccess) {
+    ocfd_batch_destroy(b);
+    return OCFD_E_CUDA;
+  }
   *out = b;
   return OCFD_OK;
 }
 
-int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
-  if (!b) return OCFD_E_PARAM;
-  // the members' streams run concurrently; each advances from its own graph
-  for (ocfd_handle* h : b->m) {
-    int r = ocfd_gpu_step(h, nsteps, 0);
-    if (r) return r;
+int ocfd_batch_set_tiles(ocfd_batch* b, const int variants[3]) {
+  if (!b || !variants) return OCFD_E_PARAM;
+  for (int d = 0; d < 3; d++) {
+    if (variants[d] < -1 || variants[d] > 1) return OCFD_E_PARAM;
+    b->forced[d] = variants[d];
   }
-  if (sync)
-    for (ocfd_handle* h : b->m) {
-      int r = ocfd_gpu_step(h, 0, 1);
-      if (r) return r;
-    }
+  b->tuned = false;
+  b->f0.clear();  // rebuild at the next step
   return OCFD_OK;
 }
 
-void ocfd_batch_destroy(ocfd_batch* b) { delete b; }
+int ocfd_batch_info(const ocfd_batch* b, int* fused, int variants[3]) {
+  if (!b) return OCFD_E_PARAM;
+  if (fused) *fused = b->fused ? 1 : 0;
+  if (variants)
+    for (int d = 0; d < 3; d++) variants[d] = b->variant[d];
+  return OCFD_OK;
+}
+
+const char* ocfd_batch_last_error(const ocfd_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
+  if (!b || nsteps < 0) return OCFD_E_PARAM;
+  if (!b->fused) {
+    // members advance concurrently on their own streams, each from its own graph
+    for (ocfd_handle* h : b->m) {
+      int r = ocfd_gpu_step(h, nsteps, 0);
+      if (r) return r;
+    }
+    if (sync)
+      for (ocfd_handle* h : b->m) {
+        int r = ocfd_gpu_sync(h);
+        if (r) return r;
+      }
+    return OCFD_OK;
+  }
+  BCK(cudaSetDevice(b->device));
+  const int n = (int)b->m.size();
+  for (int q = 0; q < n; q++) {
+    ocfd_handle* h = b->m[q];
+    if (!h->halo_valid) {
+      int r = halo_all(h);
+      if (r) return bfail(b, r, h->err);
+      h->halo_valid = true;
+    }
+    BCK(cudaEventRecord(b->ev[q], h->st));
+    BCK(cudaStreamWaitEvent(b->st, b->ev[q], 0));
+  }
+  for (int s = 0; s < nsteps; s++) {
+    // parity of every member against the tables: all 0, all 1, or rebuild
+    int par = -1;
+    bool ok = b->f0.size() == (size_t)n;
+    for (int q = 0; q < n && ok; q++) {
+      ocfd_handle* h = b->m[q];
+      const int pq = (h->f == b->f0[q] && h->prim[4] == b->t0[q]) ? 0 : (h->fn == b->f0[q] && h->talt == b->t0[q]) ? 1 : -1;
+      if (pq < 0 || (par >= 0 && pq != par)) ok = false;
+      par = pq;
+    }
+    if (!ok) {
+      int r = batch_prepare(b);
+      if (r) return r;
+      par = 0;
+    }
+    BCK(cudaGraphLaunch(b->par[par].graph, b->st));
+    for (ocfd_handle* h : b->m) {
+      std::swap(h->f, h->fn);
+      std::swap(h->prim[4], h->talt);
+      h->istep += 1;
+      h->tt += h->p.dt;
+    }
+  }
+  BCK(cudaEventRecord(b->done, b->st));
+  for (ocfd_handle* h : b->m) BCK(cudaStreamWaitEvent(h->st, b->done, 0));
+  if (sync) {
+    BCK(cudaStreamSynchronize(b->st));
+    for (ocfd_handle* h : b->m) {
+      int r = ocfd_gpu_sync(h);
+      if (r) return bfail(b, r, h->err);
+    }
+  }
+  return OCFD_OK;
+}
+
+void ocfd_batch_destroy(ocfd_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (int P = 0; P < 2; P++) {
+    if (b->par[P].graph) cudaGraphExecDestroy(b->par[P].graph);
+    if (b->par[P].dev) cudaFree(b->par[P].dev);
+  }
+  for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+}
 
 }  // extern "C"

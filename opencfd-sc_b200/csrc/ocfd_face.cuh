@@ -25,20 +25,45 @@
 
 namespace ocfd {
 
-template <int DIR>
-struct FaceTile;
+// Tile shapes (NP pencils x TF faces, NP*TF = 256).  Variant 0 is the
+// default of the single-instance launches; variant 1 (TF = 32) wastes fewer
+// threads on short pencils and is one of the choices of the batch autotuner.
+template <int DIR, int V>
+struct FaceTileV;
 template <>
-struct FaceTile<0> {
+struct FaceTileV<0, 0> {
   static constexpr int NP = 4, TF = 64;
 };
 template <>
-struct FaceTile<1> {
+struct FaceTileV<0, 1> {
+  static constexpr int NP = 8, TF = 32;
+};
+template <>
+struct FaceTileV<1, 0> {
   static constexpr int NP = 16, TF = 16;
 };
 template <>
-struct FaceTile<2> {
+struct FaceTileV<1, 1> {
+  static constexpr int NP = 8, TF = 32;
+};
+template <>
+struct FaceTileV<2, 0> {
   static constexpr int NP = 16, TF = 16;
 };
+template <>
+struct FaceTileV<2, 1> {
+  static constexpr int NP = 8, TF = 32;
+};
+template <int DIR>
+struct FaceTile : FaceTileV<DIR, 0> {};
+
+// Grid of one launch: (x, y, z) blocks for a face sweep of instance a.
+template <int DIR, int NP, int TF, typename S>
+__host__ __forceinline__ dim3 face_grid(const FaceArgs<S>& a) {
+  const int nf = a.fend - a.fbeg + 1;
+  if (DIR == 0) return dim3((nf + TF - 1) / TF, (a.g.ny + NP - 1) / NP, a.g.nz);
+  return dim3((a.g.nx + NP - 1) / NP, (nf + TF - 1) / TF, DIR == 1 ? a.g.nz : a.g.ny);
+}
 
 // ---------------------------------------------------------------------------
 // Flux-vector form, boundary-aware reconstruction of one face (OCFD2d_flux1).
@@ -184,14 +209,12 @@ struct Stencil<SCH_WENO5> {
 // ---------------------------------------------------------------------------
 // ALLIN: every face of the launch is an interior face (periodic direction), so
 // the boundary-closure paths are compiled out.
-template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
-// FP64: two resident blocks per SM (<= 128 registers) measured faster than one;
-// FP32 needs fewer registers and is faster without the cap.
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S> a) {
-  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
+// The body of one block; (bx, by, bz) are its block coordinates within the
+// instance's own launch grid.
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S>
+__device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, const int by, const int bz, R* sm) {
+  constexpr int LT = TF + 7;
   // shared memory: 10 split-flux arrays (+7 face-state arrays for CHAR)
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sm = reinterpret_cast<R*>(smem_raw);
   auto SI = [](int var, int l, int p) -> int { return var * (NP * LT) + (DIR == 0 ? p * LT + l : l * NP + p); };
 
   const Grid& G = a.g;
@@ -199,27 +222,27 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S
   const int nn = G.len(DIR);
   int g0, pbase;
   if (DIR == 0) {
-    g0 = a.fbeg + blockIdx.x * TF;
-    pbase = blockIdx.y * NP;  // NP consecutive j of plane k = blockIdx.z + 1
+    g0 = a.fbeg + bx * TF;
+    pbase = by * NP;  // NP consecutive j of plane k = bz + 1
   } else {
-    g0 = a.fbeg + blockIdx.y * TF;
-    pbase = blockIdx.x * NP;
+    g0 = a.fbeg + by * TF;
+    pbase = bx * NP;
   }
   // pencil p -> (i,j,k) with the along-direction index left at 0
   auto pencil = [&](int p, int& i, int& j, int& k) -> bool {
     if (DIR == 0) {
       i = 0;
       j = pbase + p + 1;
-      k = blockIdx.z + 1;
+      k = bz + 1;
       return j <= G.ny;
     } else if (DIR == 1) {
       i = pbase + p + 1;
       j = 0;
-      k = blockIdx.z + 1;
+      k = bz + 1;
       return i <= G.nx;
     } else {
       i = pbase + p + 1;
-      j = blockIdx.z + 1;
+      j = bz + 1;
       k = 0;
       return i <= G.nx;
     }
@@ -540,23 +563,85 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S
   }
 }
 
+// FP64: two resident blocks per SM (<= 128 registers) measured faster than one;
+// FP32 needs fewer registers and is faster without the cap.
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR>::NP, FaceTile<DIR>::TF, R, S>(
+      a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
+}
+
+// Batched launch: the blocks of all instances in one 1-D grid; each block finds
+// its instance and its block coordinates from the batch table.  Periodic
+// instances only (ALLIN).
+template <int DIR, bool CHAR, int SCHEME, int V, typename R, typename S>
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face_batch(BatchTab<FaceArgs<S>> b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int bx, by, bz;
+  const int q = batch_locate(b, blockIdx.x, bx, by, bz);
+  face_body<DIR, CHAR, SCHEME, true, FaceTileV<DIR, V>::NP, FaceTileV<DIR, V>::TF, R, S>(
+      b.args[q], bx, by, bz, reinterpret_cast<R*>(smem_raw));
+}
+
+template <int DIR, bool CHAR, int NP, int TF, typename R>
+constexpr size_t face_smem() {
+  return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R);  // split fluxes (+ face state)
+}
+
 // ---------------------------------------------------------------------------
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
 static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
-  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF, LT = TF + 7;
-  constexpr int NV = CHAR ? 17 : 10;  // split fluxes (+ face state)
-  const size_t smem = (size_t)NV * NP * LT * sizeof(R);
+  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+  constexpr size_t smem = face_smem<DIR, CHAR, NP, TF, R>();
   auto kern = k_face<DIR, CHAR, SCHEME, ALLIN, R, S>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int nf = a.fend - a.fbeg + 1;
-  dim3 grid;
-  if (DIR == 0) {
-    grid = dim3((nf + TF - 1) / TF, (a.g.ny + NP - 1) / NP, a.g.nz);
-  } else {
-    grid = dim3((a.g.nx + NP - 1) / NP, (nf + TF - 1) / TF, DIR == 1 ? a.g.nz : a.g.ny);
-  }
-  kern<<<grid, NP * TF, smem, st>>>(a);
+  kern<<<face_grid<DIR, NP, TF>(a), NP * TF, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+// Batched face sweep.  nblocks == 0 asks for the shared-memory attribute to be
+// set instead of a launch; the host fills b from face_batch_dims().
+template <int DIR, bool CHAR, int SCHEME, int V, typename R, typename S>
+static cudaError_t launch_face_batch_t(const BatchTab<FaceArgs<S>>& b, int nblocks, cudaStream_t st) {
+  constexpr int NP = FaceTileV<DIR, V>::NP, TF = FaceTileV<DIR, V>::TF;
+  constexpr size_t smem = face_smem<DIR, CHAR, NP, TF, R>();
+  auto kern = k_face_batch<DIR, CHAR, SCHEME, V, R, S>;
+  if (nblocks == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<nblocks, NP * TF, smem, st>>>(b);
+  return cudaGetLastError();
+}
+
+template <typename R, typename S>
+cudaError_t launch_face_batch(int dir, bool chr, int scheme, int variant, const BatchTab<FaceArgs<S>>& b,
+                              int nblocks, cudaStream_t st) {
+#define OCFD_FB_CASE(D, C, SC)                                                     \
+  if (dir == D && chr == C && scheme == SC)                                        \
+    return variant ? launch_face_batch_t<D, C, SC, 1, R, S>(b, nblocks, st)        \
+                   : launch_face_batch_t<D, C, SC, 0, R, S>(b, nblocks, st);
+#define OCFD_FB_SCHEMES(D, C) \
+  OCFD_FB_CASE(D, C, SCH_WENO5) \
+  OCFD_FB_CASE(D, C, SCH_WENO7) \
+  OCFD_FB_CASE(D, C, SCH_OMP6)  \
+  OCFD_FB_CASE(D, C, SCH_UD7L)  \
+  OCFD_FB_CASE(D, C, SCH_HYBRID)
+  OCFD_FB_SCHEMES(0, false)
+  OCFD_FB_SCHEMES(1, false)
+  OCFD_FB_SCHEMES(2, false)
+  OCFD_FB_SCHEMES(0, true)
+  OCFD_FB_SCHEMES(1, true)
+  OCFD_FB_SCHEMES(2, true)
+#undef OCFD_FB_SCHEMES
+#undef OCFD_FB_CASE
+  return cudaErrorInvalidValue;
+}
+
+// Per-instance launch grid of a batched face sweep for tile variant V.
+template <typename S>
+dim3 face_batch_dims(int dir, int variant, const FaceArgs<S>& a) {
+  if (dir == 0) return variant ? face_grid<0, 8, 32>(a) : face_grid<0, 4, 64>(a);
+  if (dir == 1) return variant ? face_grid<1, 8, 32>(a) : face_grid<1, 16, 16>(a);
+  return variant ? face_grid<2, 8, 32>(a) : face_grid<2, 16, 16>(a);
 }
 
 template <typename R, typename S>

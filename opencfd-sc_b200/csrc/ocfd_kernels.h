@@ -67,10 +67,48 @@ struct PtrList {
   int n;
 };
 
+// Table of a batched launch (several instances, one kernel launch): per
+// instance its argument block and {first linear block of its part of the grid,
+// that part's x extent, its y extent, unused}.  Both arrays live on the device.
+template <typename A>
+struct BatchTab {
+  const A* args;
+  const int4* ent;
+  int count;
+};
+// The instance owning linear block lin, and the block's (x, y, z) coordinates
+// within that instance's grid (binary search over the first blocks).
+template <typename A>
+__device__ __forceinline__ int batch_locate(const BatchTab<A>& b, int lin, int& bx, int& by, int& bz) {
+  int lo = 0, hi = b.count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&b.ent[mid].x) <= lin)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const int4 e = __ldg(&b.ent[lo]);
+  int l = lin - e.x;
+  bx = l % e.y;
+  l /= e.y;
+  by = l % e.z;
+  bz = l / e.z;
+  return lo;
+}
+
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st);
+template <typename R, typename S>
+cudaError_t launch_face_batch(int dir, bool chr, int scheme, int variant, const BatchTab<FaceArgs<S>>& b,
+                              int nblocks, cudaStream_t st);
+template <typename S>
+dim3 face_batch_dims(int dir, int variant, const FaceArgs<S>& a);
 // raise the dynamic shared-memory limit of every face kernel (call outside graph capture)
 cudaError_t setup_face_kernels();
+// shared-memory limits of the batched face kernels (once per device, before the first batch launch)
+cudaError_t setup_face_batch_kernels_f64();
+cudaError_t setup_face_batch_kernels_f32();
 
 template <typename R, typename S>
 cudaError_t launch_visc_grad(const ViscArgs<R, S>& a, cudaStream_t st);
@@ -91,6 +129,15 @@ cudaError_t launch_rk3(const Grid& g, double* f, const double* fn, const double*
 cudaError_t launch_duvwt(const UpdArgs<double>& a, cudaStream_t st);
 // serial in-order repair of the points with T <= 0 (handle_NegativeT)
 cudaError_t launch_negt_fix(const UpdArgs<double>& a, cudaStream_t st);
+// Batched versions (one launch for all instances of a BatchTab; the grid of an
+// instance is that of the single launch, see update_dims()).
+template <typename R, typename S>
+cudaError_t launch_visc_grad_batch(const BatchTab<ViscArgs<R, S>>& b, int nblocks, cudaStream_t st);
+template <typename R>
+cudaError_t launch_fused_batch(const BatchTab<UpdArgs<R>>& b, int nblocks, bool chr, bool visc, bool fuse_bc,
+                               cudaStream_t st);
+cudaError_t launch_negt_fix_batch(const BatchTab<UpdArgs<double>>& b, cudaStream_t st);
+inline dim3 update_dims(const Grid& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
 
 // periodic face halo of narr haloed arrays (exchange_boundary_xyz)
 cudaError_t launch_halo(const Grid& g, const int periodic[3], PtrList<double> arrs, cudaStream_t st);

@@ -59,11 +59,11 @@ __device__ __forceinline__ R d0(F at, int l, int nn, int periodic, int cd8, D0C<
 // du_viscous part 1 (OCFD_viscous.f90:193-264): comput_Amu (:135-149), the 12
 // gradients, stress and heat flux, and the contravariant viscous fluxes Ev.
 template <typename R, typename S>
-__global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
+__device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const int bx, const int by, const int bz) {
   const Grid& G = a.g;
-  const int i = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
-  const int j = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
-  const int k = blockIdx.z + 1;
+  const int i = bx * 32 + (threadIdx.x & 31) + 1;
+  const int j = by * 8 + (threadIdx.x >> 5) + 1;
+  const int k = bz + 1;
   if (i > G.nx || j > G.ny) return;
   const long long c = G.ih(i, j, k);
   const int cd8 = a.ph.scheme_vis == 6;
@@ -126,13 +126,31 @@ __global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
 }
 
 template <typename R, typename S>
+__global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
+  visc_grad_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R, typename S>
+__global__ void __launch_bounds__(256) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
+  int bx, by, bz;
+  const int q = batch_locate(b, blockIdx.x, bx, by, bz);
+  visc_grad_body(b.args[q], bx, by, bz);
+}
+
+template <typename R, typename S>
 cudaError_t launch_visc_grad(const ViscArgs<R, S>& a, cudaStream_t st) {
-  dim3 grid((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, a.g.nz);
-  k_visc_grad<R, S><<<grid, 256, 0, st>>>(a);
+  k_visc_grad<R, S><<<update_dims(a.g), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <typename R, typename S>
+cudaError_t launch_visc_grad_batch(const BatchTab<ViscArgs<R, S>>& b, int nblocks, cudaStream_t st) {
+  k_visc_grad_batch<R, S><<<nblocks, 256, 0, st>>>(b);
   return cudaGetLastError();
 }
 template cudaError_t launch_visc_grad<double, double>(const ViscArgs<double, double>&, cudaStream_t);
 template cudaError_t launch_visc_grad<float, float>(const ViscArgs<float, float>&, cudaStream_t);
+template cudaError_t launch_visc_grad_batch<double, double>(const BatchTab<ViscArgs<double, double>>&, int,
+                                                           cudaStream_t);
+template cudaError_t launch_visc_grad_batch<float, float>(const BatchTab<ViscArgs<float, float>>&, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Flux difference of the three sweeps into du (OCFD_inviscous.f90:106-108,
@@ -303,11 +321,11 @@ __global__ void __launch_bounds__(256) k_visc_div(UpdArgs<R> a) {
 
 // The fused stage tail.
 template <bool CHAR, bool VISC, bool FUSEBC, typename R>
-__global__ void __launch_bounds__(256) k_fused(UpdArgs<R> a) {
+__device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, const int by, const int bz) {
   const Grid& G = a.g;
-  const int i = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
-  const int j = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
-  const int k = blockIdx.z + 1;
+  const int i = bx * 32 + (threadIdx.x & 31) + 1;
+  const int j = by * 8 + (threadIdx.x >> 5) + 1;
+  const int k = bz + 1;
   if (i > G.nx || j > G.ny) return;
   R du[5];
   inv_div<CHAR>(a, i, j, k, du);
@@ -350,6 +368,17 @@ __global__ void __launch_bounds__(256) k_fused(UpdArgs<R> a) {
   }
 }
 
+template <bool CHAR, bool VISC, bool FUSEBC, typename R>
+__global__ void __launch_bounds__(256) k_fused(UpdArgs<R> a) {
+  fused_body<CHAR, VISC, FUSEBC, R>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <bool CHAR, bool VISC, bool FUSEBC, typename R>
+__global__ void __launch_bounds__(256) k_fused_batch(BatchTab<UpdArgs<R>> b) {
+  int bx, by, bz;
+  const int q = batch_locate(b, blockIdx.x, bx, by, bz);
+  fused_body<CHAR, VISC, FUSEBC, R>(b.args[q], bx, by, bz);
+}
+
 template <typename R>
 cudaError_t launch_div_inv(const UpdArgs<R>& a, cudaStream_t st) {
   dim3 grid((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, a.g.nz);
@@ -381,6 +410,24 @@ cudaError_t launch_fused(const UpdArgs<R>& a, cudaStream_t st) {
 #undef OCFD_FUSED
   return cudaGetLastError();
 }
+template <typename R>
+cudaError_t launch_fused_batch(const BatchTab<UpdArgs<R>>& b, int nblocks, bool chr, bool visc, bool fuse_bc,
+                               cudaStream_t st) {
+#define OCFD_FUSED(C, V, B) \
+  if (chr == C && visc == V && fuse_bc == B) k_fused_batch<C, V, B, R><<<nblocks, 256, 0, st>>>(b);
+  OCFD_FUSED(false, false, false)
+  OCFD_FUSED(false, false, true)
+  OCFD_FUSED(false, true, false)
+  OCFD_FUSED(false, true, true)
+  OCFD_FUSED(true, false, false)
+  OCFD_FUSED(true, false, true)
+  OCFD_FUSED(true, true, false)
+  OCFD_FUSED(true, true, true)
+#undef OCFD_FUSED
+  return cudaGetLastError();
+}
+template cudaError_t launch_fused_batch<double>(const BatchTab<UpdArgs<double>>&, int, bool, bool, bool, cudaStream_t);
+template cudaError_t launch_fused_batch<float>(const BatchTab<UpdArgs<float>>&, int, bool, bool, bool, cudaStream_t);
 template cudaError_t launch_div_inv<double>(const UpdArgs<double>&, cudaStream_t);
 template cudaError_t launch_div_inv<float>(const UpdArgs<float>&, cudaStream_t);
 template cudaError_t launch_visc_div<double>(const UpdArgs<double>&, cudaStream_t);
@@ -438,8 +485,7 @@ cudaError_t launch_duvwt(const UpdArgs<double>& a, cudaStream_t st) {
 // in place while sweeping, so a neighbour earlier in the sweep contributes its
 // new value and a later neighbour (or a halo cell) the value of the previous
 // stage, kept in told.  More than 10 points: the reference stops (:13-16).
-__global__ void k_negt_fix(UpdArgs<double> a) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void negt_fix_body(const UpdArgs<double>& a) {
   DevStatus* st = a.st;
   const int cnt = st->negt_count;
   st->negt_last = cnt;
@@ -487,8 +533,21 @@ __global__ void k_negt_fix(UpdArgs<double> a) {
     }
   }
 }
+__global__ void k_negt_fix(UpdArgs<double> a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  negt_fix_body(a);
+}
+// one block per instance
+__global__ void k_negt_fix_batch(BatchTab<UpdArgs<double>> b) {
+  if (threadIdx.x != 0 || (int)blockIdx.x >= b.count) return;
+  negt_fix_body(b.args[blockIdx.x]);
+}
 cudaError_t launch_negt_fix(const UpdArgs<double>& a, cudaStream_t st) {
   k_negt_fix<<<1, 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_negt_fix_batch(const BatchTab<UpdArgs<double>>& b, cudaStream_t st) {
+  k_negt_fix_batch<<<b.count, 32, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -95,6 +95,12 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_batch_step.restype = C.c_int
     L.ocfd_batch_destroy.argtypes = [H]
     L.ocfd_batch_destroy.restype = None
+    L.ocfd_batch_set_tiles.argtypes = [H, C.POINTER(C.c_int)]
+    L.ocfd_batch_set_tiles.restype = C.c_int
+    L.ocfd_batch_info.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.ocfd_batch_info.restype = C.c_int
+    L.ocfd_batch_last_error.argtypes = [H]
+    L.ocfd_batch_last_error.restype = C.c_char_p
     L.ocfd_show_flow_msg_noalloc.argtypes = [P, C.c_void_p, C.c_void_p * 5, C.c_void_p, C.c_void_p, dp]
     L.ocfd_show_flow_msg_noalloc.restype = C.c_int
     return L
@@ -121,4 +127,5 @@ EXPORTED = [
     "ocfd_gpu_du_viscous", "ocfd_gpu_rk3", "ocfd_gpu_duvwt", "ocfd_gpu_bc", "ocfd_gpu_filter",
     "ocfd_gpu_advance_clock", "ocfd_gpu_step", "ocfd_gpu_show_flow_msg", "ocfd_gpu_ana_box", "ocfd_batch_create",
     "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps", "ocfd_show_flow_msg_noalloc",
+    "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error",
 ]

@@ -228,3 +228,54 @@ class Solver:
     @property
     def mixed(self) -> bool:
         return self.p.precision == PRECISION_MIXED
+
+
+class Batch:
+    """Several solver instances advanced together (ocfd_batch_*): one launch per
+    kernel and RK stage for all of them when their configuration allows it,
+    bit-identical to stepping each alone."""
+
+    def __init__(self, members: list[Solver]):
+        if not members:
+            raise ValueError("empty batch")
+        self.members = list(members)
+        self.L = members[0].L
+        hs = (C.c_void_p * len(members))(*[m.h for m in members])
+        b = C.c_void_p()
+        r = self.L.ocfd_batch_create(C.cast(hs, C.POINTER(C.c_void_p)), len(members), C.byref(b))
+        if r != 0:
+            raise _lib.OcfdError(r, "ocfd_batch_create failed")
+        self.b = b
+
+    def _check(self, r: int, what: str):
+        if r == 0:
+            return
+        msg = self.L.ocfd_batch_last_error(self.b)
+        msg = msg.decode() if msg else ""
+        if r == _lib.OCFD_E_NEGT:
+            raise _lib.NegativeTemperatureStop(r, msg or what)
+        raise _lib.OcfdError(r, f"{what}: {msg}")
+
+    def step(self, n: int = 1, sync: bool = True):
+        self._check(self.L.ocfd_batch_step(self.b, n, 1 if sync else 0), "batch_step")
+
+    def set_tiles(self, variants):
+        v = (C.c_int * 3)(*variants)
+        self._check(self.L.ocfd_batch_set_tiles(self.b, v), "batch_set_tiles")
+
+    def info(self):
+        fused = C.c_int()
+        v = (C.c_int * 3)()
+        self._check(self.L.ocfd_batch_info(self.b, C.byref(fused), v), "batch_info")
+        return bool(fused.value), list(v)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.ocfd_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -341,6 +341,72 @@ def run_ours(args):
     return 0
 
 
+def run_serve(args):
+    """Served mixed-precision stream (continuous batching) against sequential plain
+    FP64 solves of the same requests.  The error of the served results against
+    the FP64 ones is stated on a sample of requests beside the predictability
+    floor of each flow: the FP64 solve from an initial field perturbed by one
+    FP32 rounding (relative 2^-24), since at these Reynolds numbers and step
+    counts the flows are chaotic and any rounding difference grows."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    from ocfd_b200 import serving
+
+    reqs = serving.make_stream(args.requests, rate=args.rate, seed=20261203)
+    sample = [r.rid for r in reqs[:: max(1, len(reqs) // 16)]]
+    # the requests arrive with their initial fields (prepared before the stream starts)
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        prepared = list(ex.map(lambda r: serving.request_setup(r, True), reqs))
+    payloads = {r.rid: x for r, x in zip(reqs, prepared)}
+    srv = serving.Server(mixed=True, round_steps=args.round_steps, keep=sample)
+    served = srv.run(reqs, realtime=True, payloads=payloads)
+    seq = serving.run_sequential(reqs, mixed=False, keep=sample, payloads=payloads)
+
+    inner = (slice(4, -4),) * 3
+
+    def errors(a_state, a_E0, b_state, b_E0, ma):
+        (fa, pa), (fb, pb) = a_state, b_state
+        rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+        pr = lambda P: P[0][inner] * P[4][inner] / (1.4 * ma * ma)
+        return {"ke": abs(a_E0[1] - b_E0[1]) / abs(b_E0[1]), "rho": rel(pa[0][inner], pb[0][inner]),
+                "u": max(rel(pa[q][inner], pb[q][inner]) for q in (1, 2, 3)), "p": rel(pr(pa), pr(pb))}
+
+    mixed_err, floor_err = [], []
+    rng = np.random.default_rng(5)
+    for rid in sample:
+        r = reqs[rid]
+        b = seq["results"][rid]
+        a = served["results"][rid]
+        mixed_err.append(errors(a.state, a.E0, b.state, b.E0, r.ma))
+        p, xyz, prims = payloads[rid]
+        p = p.copy()
+        p.precision = 0
+        pert = [prims[0]] + [q * (1.0 + 2.0 ** -24 * rng.standard_normal(q.shape)) for q in prims[1:]]
+        s = serving._start(p, xyz, pert, 0)
+        s.step(r.steps)
+        floor_err.append(errors(s.download_state(), s.show_flow_msg().tolist(), b.state, b.E0, r.ma))
+        s.close()
+    agg = lambda L: {f"{k}_rel_max": max(e[k] for e in L) for k in ("ke", "rho", "u", "p")} | {
+        f"{k}_rel_median": float(np.median([e[k] for e in L])) for k in ("ke", "u")}
+    work = sum(r.n ** 3 * r.steps for r in reqs)
+    line = {
+        "metric": "served stream: aggregate GPts/s and p50/p99 time-to-result, mixed precision, continuous batching",
+        "mode": "serve", "requests": len(reqs), "rate_per_s": args.rate, "work_gpt_steps": work,
+        "data": "synthetic (seeded Poisson stream of TGV / isotropic-turbulence requests, sizes 32^3-128^3)",
+        "served_mixed": {k: served[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s", "rounds", "batched_rounds",
+                                                 "max_active")},
+        "sequential_fp64": {k: seq[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s", "wall_s")},
+        "throughput_ratio": served["gpts_per_s"] / seq["gpts_per_s"],
+        "error_vs_fp64": {"sample": len(sample), **agg(mixed_err)},
+        "fp64_perturbed_2^-24_vs_fp64": agg(floor_err),
+        "scheme": "WENO7 flux-vector, SW, CD6; dt at CFL 0.5 from the initial field",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,11 +416,17 @@ def main():
     ap.add_argument("--workload", default="tgv256_omp6_char", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--serve", action="store_true", help="served request stream instead of the step benchmark")
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--round-steps", type=int, default=25)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve:
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -578,10 +578,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S
 template <int DIR, bool CHAR, int SCHEME, int V, typename R, typename S>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face_batch(BatchTab<FaceArgs<S>> b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(16) FaceArgs<S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
   face_body<DIR, CHAR, SCHEME, true, FaceTileV<DIR, V>::NP, FaceTileV<DIR, V>::TF, R, S>(
-      b.args[q], bx, by, bz, reinterpret_cast<R*>(smem_raw));
+      batch_args(b, q, &sa), bx, by, bz, reinterpret_cast<R*>(smem_raw));
 }
 
 template <int DIR, bool CHAR, int NP, int TF, typename R>

@@ -97,6 +97,19 @@ __device__ __forceinline__ int batch_locate(const BatchTab<A>& b, int lin, int& 
   return lo;
 }
 
+// Copies instance q's argument block into shared memory (the block's threads
+// share it; reads from shared memory do not alias the kernel's global stores,
+// so the compiler need not keep every field in registers).
+template <typename A>
+__device__ __forceinline__ const A& batch_args(const BatchTab<A>& b, int q, A* sa) {
+  static_assert(sizeof(A) % 4 == 0, "argument blocks are copied as 4-byte words");
+  const int* src = reinterpret_cast<const int*>(b.args + q);
+  int* dst = reinterpret_cast<int*>(sa);
+  for (int t = threadIdx.x; t < (int)(sizeof(A) / 4); t += blockDim.x) dst[t] = __ldg(src + t);
+  __syncthreads();
+  return *sa;
+}
+
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st);
 template <typename R, typename S>

@@ -131,9 +131,10 @@ __global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
 }
 template <typename R, typename S>
 __global__ void __launch_bounds__(256) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
+  __shared__ __align__(16) ViscArgs<R, S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
-  visc_grad_body(b.args[q], bx, by, bz);
+  visc_grad_body(batch_args(b, q, &sa), bx, by, bz);
 }
 
 template <typename R, typename S>
@@ -374,9 +375,10 @@ __global__ void __launch_bounds__(256) k_fused(UpdArgs<R> a) {
 }
 template <bool CHAR, bool VISC, bool FUSEBC, typename R>
 __global__ void __launch_bounds__(256) k_fused_batch(BatchTab<UpdArgs<R>> b) {
+  __shared__ __align__(16) UpdArgs<R> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
-  fused_body<CHAR, VISC, FUSEBC, R>(b.args[q], bx, by, bz);
+  fused_body<CHAR, VISC, FUSEBC, R>(batch_args(b, q, &sa), bx, by, bz);
 }
 
 template <typename R>

@@ -58,15 +58,18 @@ def tgv_prims(p: OcfdParams):
     """TGV initial primitives: rho=1, u=sin x cos y cos z, v=-cos x sin y cos z, w=0,
     p = p0 + (cos2x+cos2y)(cos2z+2)/16, T = p/(rho p0), p0 = 1/(gamma Ma^2)."""
     x, y, z = box_coords(p.nx, p.ny, p.nz)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    # the trigonometric factors are evaluated on the 1-D coordinates and
+    # broadcast (the same values and products as on the full 3-D mesh)
+    X, Y, Z = x[None, None, :], y[None, :, None], z[:, None, None]
+    shape = (p.nz, p.ny, p.nx)
     p0 = 1.0 / (p.gamma * p.ma * p.ma)
-    d = np.ones_like(X)
+    d = np.ones(shape)
     u = np.sin(X) * np.cos(Y) * np.cos(Z)
     v = -np.cos(X) * np.sin(Y) * np.cos(Z)
-    w = np.zeros_like(X)
+    w = np.zeros(shape)
     pr = p0 + (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0) / 16.0
     T = pr / (d * p0)
-    return [np.ascontiguousarray(a) for a in (d, u, v, w, T)]
+    return [np.ascontiguousarray(np.broadcast_to(a, shape)) for a in (d, u, v, w, T)]
 
 
 def hit_params(n: int, re: float = 500.0, ma: float = 1.0, dt: float = 1e-3, steps: int = 300,

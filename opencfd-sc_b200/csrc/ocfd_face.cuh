@@ -563,10 +563,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   }
 }
 
-// FP64: two resident blocks per SM (<= 128 registers) measured faster than one;
-// FP32 needs fewer registers and is faster without the cap.
+// Minimum resident blocks per SM.  FP64: two (<= 128 registers) measured
+// faster than one.  FP32: four (<= 64 registers) -- 17% faster than two on the
+// characteristic OMP6 sweeps at 256^3 despite a few spilled registers, equal on
+// the flux-vector sweeps.
+#ifndef OCFD_FACE32_MINB
+#define OCFD_FACE32_MINB 4
+#endif
+#define OCFD_FACE_MINB (sizeof(R) == 8 ? 2 : OCFD_FACE32_MINB)
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S> a) {
+__global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face(FaceArgs<S> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR>::NP, FaceTile<DIR>::TF, R, S>(
       a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face(FaceArgs<S
 // its instance and its block coordinates from the batch table.  Periodic
 // instances only (ALLIN).
 template <int DIR, bool CHAR, int SCHEME, int V, typename R, typename S>
-__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 2 : 1) k_face_batch(BatchTab<FaceArgs<S>> b) {
+__global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<FaceArgs<S>> b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(16) FaceArgs<S> sa;
   int bx, by, bz;

@@ -11,6 +11,18 @@
 #include "ocfd_kernels.h"
 #include "ocfd_schemes.cuh"
 
+// Minimum resident blocks per SM requested for the viscous-gradient and
+// stage-tail kernels (both memory-latency bound: more resident warps keep
+// more loads in flight, at the price of registers).  Measured best on B200 at
+// 256^3: FP64 tail 5, FP32 tail 6, FP64 viscous 4, FP32 viscous 6 (against
+// 2-3 blocks with the compiler's own register choice).
+#ifndef OCFD_VISC_MINB
+#define OCFD_VISC_MINB (sizeof(R) == 8 ? 4 : 6)
+#endif
+#ifndef OCFD_TAIL_MINB
+#define OCFD_TAIL_MINB (sizeof(R) == 8 ? 5 : 6)
+#endif
+
 namespace ocfd {
 
 // ---------------------------------------------------------------------------
@@ -126,11 +138,11 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
 }
 
 template <typename R, typename S>
-__global__ void __launch_bounds__(256) k_visc_grad(ViscArgs<R, S> a) {
+__global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad(ViscArgs<R, S> a) {
   visc_grad_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R, typename S>
-__global__ void __launch_bounds__(256) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
+__global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
   __shared__ __align__(16) ViscArgs<R, S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
@@ -370,11 +382,11 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
 }
 
 template <bool CHAR, bool VISC, bool FUSEBC, typename R>
-__global__ void __launch_bounds__(256) k_fused(UpdArgs<R> a) {
+__global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused(UpdArgs<R> a) {
   fused_body<CHAR, VISC, FUSEBC, R>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <bool CHAR, bool VISC, bool FUSEBC, typename R>
-__global__ void __launch_bounds__(256) k_fused_batch(BatchTab<UpdArgs<R>> b) {
+__global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused_batch(BatchTab<UpdArgs<R>> b) {
   __shared__ __align__(16) UpdArgs<R> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);

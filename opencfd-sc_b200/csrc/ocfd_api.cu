@@ -110,6 +110,11 @@ void fill_phys(const ocfd_params& p, Phys& ph, DCoef& dc) {
   ph.kb2 = p.kb2;
   ph.ibc = p.ibc;
   ph.bc_para0 = p.bc_para[0];
+  ph.inv_ma = 1.0 / p.ma;
+  ph.inv_2g = 1.0 / (2.0 * p.gamma);
+  ph.inv_g = 1.0 / p.gamma;
+  ph.inv_gm1 = 1.0 / (p.gamma - 1.0);
+  ph.sw_tmp3 = (3.0 - p.gamma) / (2.0 * (p.gamma - 1.0));
   // OCFD_dxyz_viscous.f90:9-16
   const double hh[3] = {p.hx, p.hy, p.hz};
   for (int d = 0; d < 3; d++) {

@@ -59,22 +59,53 @@ struct Phys {
   int ibc;
   int ghost[6];
   double bc_para0;
+  // reciprocals precomputed on the host for the production build
+  double inv_ma;    // 1/Ma
+  double inv_2g;    // 1/(2 gamma)
+  double inv_g;     // 1/gamma
+  double inv_gm1;   // 1/(gamma-1)
+  double sw_tmp3;   // (3-gamma)/(2(gamma-1))
 };
+
+// The production build replaces divisions by multiplications with a shared or
+// precomputed reciprocal (results move by a few ulp; an FP64 division costs
+// about ten FP64-pipe instructions).  The strict build keeps every division of
+// the reference, in order, for bit-identical parity with the oracle.
+#ifdef OCFD_STRICT
+#define OCFD_FEWER_DIVS 0
+#else
+#define OCFD_FEWER_DIVS 1
+#endif
 
 // Steger-Warming splitting of one point: split_Stager_Warming,
 // OCFD_flux_split.f90:5-70 (the P2 term is dropped there, :51-60).
 template <typename R>
-__device__ __forceinline__ void split_sw(R g, R c, R d, R u, R v, R w, R A1, R A2, R A3, R* fp, R* fm) {
+__device__ __forceinline__ void split_sw(const Phys& ph, R g, R c, R d, R u, R v, R w, R A1, R A2, R A3, R* fp,
+                                         R* fm) {
   const R tmp1 = R(2) * (g - R(1));
+#if OCFD_FEWER_DIVS
+  const R tmp3 = R(ph.sw_tmp3);
+#else
   const R tmp3 = (R(3) - g) / (R(2) * (g - R(1)));
+#endif
+#if OCFD_FEWER_DIVS
+  const R s2 = A1 * A1 + A2 * A2 + A3 * A3;
+  R ss1 = rsqrt(s2);
+  R ss = s2 * ss1;
+#else
   R ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
   R ss1 = R(1) / ss;
+#endif
   R ak1 = A1 * ss1, ak2 = A2 * ss1, ak3 = A3 * ss1;
   R vs = A1 * u + A2 * v + A3 * w;
   R E1 = vs, E2 = vs - c * ss, E3 = vs + c * ss;
   R E1P = (E1 + fabs(E1)) * R(0.5), E2P = (E2 + fabs(E2)) * R(0.5), E3P = (E3 + fabs(E3)) * R(0.5);
   R E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
+#if OCFD_FEWER_DIVS
+  R tmp0 = d * R(ph.inv_2g);
+#else
   R tmp0 = d / (R(2) * g);
+#endif
   R uc1 = u - c * ak1, uc2 = u + c * ak1;
   R vc1 = v - c * ak2, vc2 = v + c * ak2;
   R wc1 = w - c * ak3, wc2 = w + c * ak3;
@@ -97,9 +128,15 @@ __device__ __forceinline__ void split_sw(R g, R c, R d, R u, R v, R w, R A1, R A
 // Local Lax-Friedrichs splitting of one point (eigenvalue bound per point):
 // split_Local_LaxFriedrichs, OCFD_flux_split.f90:73-104.
 template <typename R>
-__device__ __forceinline__ void split_llf(R g, R c, R d, R u, R v, R w, R A1, R A2, R A3, R* fp, R* fm) {
+__device__ __forceinline__ void split_llf(const Phys& ph, R g, R c, R d, R u, R v, R w, R A1, R A2, R A3, R* fp,
+                                          R* fm) {
+#if OCFD_FEWER_DIVS
+  const R tmp0 = R(ph.inv_g);
+  const R tmp1 = R(ph.inv_gm1);
+#else
   const R tmp0 = R(1) / g;
   const R tmp1 = R(1) / (g - R(1));
+#endif
   R ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
   R un = A1 * u + A2 * v + A3 * w;
   R lamda0 = fabs(un) + ss * c;

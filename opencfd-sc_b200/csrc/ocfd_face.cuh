@@ -276,12 +276,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       A2 = R(__ldg(a.A2 + h));
       A3 = R(__ldg(a.A3 + h));
     }
+#if OCFD_FEWER_DIVS
+    const R c = sqrt(T) * R(ph.inv_ma);
+#else
     const R c = sqrt(T) / ma;  // cc: OCFD_inviscous.f90:67
+#endif
     R fp[5], fm[5];
     if (a.split == 1)
-      split_sw(gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+      split_sw(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
     else
-      split_llf(gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+      split_llf(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
 #pragma unroll
     for (int m = 0; m < 5; m++) {
       sm[SI(m, l, p)] = fp[m];
@@ -412,28 +416,52 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         const R a2 = (W(15, 3) + W(15, 4)) * R(0.5);
         const R a3 = (W(16, 3) + W(16, 4)) * R(0.5);
         // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
+#if OCFD_FEWER_DIVS
+        const R rs = rsqrt(a1 * a1 + a2 * a2 + a3 * a3);
+        const R n1 = a1 * rs, n2 = a2 * rs, n3 = a3 * rs;
+#else
         R ss = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
         const R n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
+#endif
         R l1, l2, l3;
         if (fabs(n3) <= fabs(n2)) {
+#if OCFD_FEWER_DIVS
+          const R rl = rsqrt(n1 * n1 + n2 * n2);
+          l1 = -n2 * rl;
+          l2 = n1 * rl;
+#else
           ss = sqrt(n1 * n1 + n2 * n2);
           l1 = -n2 / ss;
           l2 = n1 / ss;
+#endif
           l3 = R(0);
         } else {
+#if OCFD_FEWER_DIVS
+          const R rl = rsqrt(n1 * n1 + n3 * n3);
+          l1 = -n3 * rl;
+          l3 = n1 * rl;
+#else
           ss = sqrt(n1 * n1 + n3 * n3);
           l1 = -n3 / ss;
-          l2 = R(0);
           l3 = n1 / ss;
+#endif
+          l2 = R(0);
         }
         const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
         const R un = u1 * n1 + v1 * n2 + w1 * n3;
         const R ul = u1 * l1 + v1 * l2 + w1 * l3;
         const R um = u1 * m1 + v1 * m2 + w1 * m3;
         const R V2 = (u1 * u1 + v1 * v1 + w1 * w1) * R(0.5);
+#if OCFD_FEWER_DIVS
+        const R rc = R(1) / c1;
+        const R KK = (R(ph.gamma) - R(1)) * (rc * rc);
+        const R KK1 = KK * R(0.5);
+        const R X1 = R(0.5) * rc;
+#else
         const R KK = (R(ph.gamma) - R(1)) / (c1 * c1);
         const R KK1 = KK * R(0.5);
         const R X1 = R(1) / (R(2) * c1);
+#endif
         const R L[5][5] = {{R(1) - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
                            {-ul, l1, l2, l3, R(0)},
                            {-um, m1, m2, m3, R(0)},

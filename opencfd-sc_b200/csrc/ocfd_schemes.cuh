@@ -16,6 +16,55 @@ namespace ocfd {
 template <typename R>
 __device__ __forceinline__ R sq(R x) { return x * x; }
 
+#ifndef OCFD_FEWER_DIVS
+#ifdef OCFD_STRICT
+#define OCFD_FEWER_DIVS 0
+#else
+#define OCFD_FEWER_DIVS 1
+#endif
+#endif
+
+// Normalised WENO sum (a0 q0 + ...) / (a0 + ...) with a_k = C_k / (ep + S_k)^2,
+// in the reference's order.  Production FP64 build: every a_k is multiplied by
+// the product of all (ep + S_j)^2, a'_k = C_k prod_{j != k} (ep + S_j)^2, which
+// leaves the normalised weights unchanged and needs one division instead of
+// one per candidate plus one.  (ep + S)^2 >= ep^2, and the indicators of
+// physical fluxes keep the products far inside the double range; FP32, whose
+// range is too small for the products, keeps the reference form.
+template <typename R>
+__device__ __forceinline__ R weno_sum3(R ep, R C0, R C1, R C2, R S0, R S1, R S2, R q0, R q1, R q2) {
+#if OCFD_FEWER_DIVS
+  if (sizeof(R) == 8) {
+    const R D0 = sq(ep + S0), D1 = sq(ep + S1), D2 = sq(ep + S2);
+    const R w0 = C0 * (D1 * D2), w1 = C1 * (D0 * D2), w2 = C2 * (D0 * D1);
+    return (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
+  }
+#endif
+  R a0 = C0 / sq(ep + S0);
+  R a1 = C1 / sq(ep + S1);
+  R a2 = C2 / sq(ep + S2);
+  R am = a0 + a1 + a2;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / am;
+}
+template <typename R>
+__device__ __forceinline__ R weno_sum4(R ep, R C0, R C1, R C2, R C3, R S0, R S1, R S2, R S3, R q0, R q1, R q2,
+                                       R q3) {
+#if OCFD_FEWER_DIVS
+  if (sizeof(R) == 8) {
+    const R D0 = sq(ep + S0), D1 = sq(ep + S1), D2 = sq(ep + S2), D3 = sq(ep + S3);
+    const R P01 = D0 * D1, P23 = D2 * D3;
+    const R w0 = C0 * (D1 * P23), w1 = C1 * (D0 * P23), w2 = C2 * (P01 * D3), w3 = C3 * (P01 * D2);
+    return (w0 * q0 + w1 * q1 + w2 * q2 + w3 * q3) / (w0 + w1 + w2 + w3);
+  }
+#endif
+  R a0 = C0 / sq(ep + S0);
+  R a1 = C1 / sq(ep + S1);
+  R a2 = C2 / sq(ep + S2);
+  R a3 = C3 / sq(ep + S3);
+  R am = a0 + a1 + a2 + a3;
+  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / am;
+}
+
 template <typename R>
 __device__ __forceinline__ R sign1(R b) { return copysign(R(1), b); }
 
@@ -32,14 +81,10 @@ __device__ __forceinline__ R weno5P(const R* v) {
   R S0 = k1312 * sq(v[0] - R(2) * v[1] + v[2]) + k14 * sq(R(3) * v[0] - R(4) * v[1] + v[2]);
   R S1 = k1312 * sq(v[-1] - R(2) * v[0] + v[1]) + k14 * sq(v[-1] - v[1]);
   R S2 = k1312 * sq(v[-2] - R(2) * v[-1] + v[0]) + k14 * sq(v[-2] - R(4) * v[-1] + R(3) * v[0]);
-  R a0 = C03 / sq(ep + S0);
-  R a1 = C13 / sq(ep + S1);
-  R a2 = C23 / sq(ep + S2);
-  R am = a0 + a1 + a2;
   R q03 = R(1.0 / 3.0) * v[0] + R(5.0 / 6.0) * v[1] - R(1.0 / 6.0) * v[2];
   R q13 = R(-1.0 / 6.0) * v[-1] + R(5.0 / 6.0) * v[0] + R(1.0 / 3.0) * v[1];
   R q23 = R(1.0 / 3.0) * v[-2] - R(7.0 / 6.0) * v[-1] + R(11.0 / 6.0) * v[0];
-  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+  return weno_sum3(ep, C03, C13, C23, S0, S1, S2, q03, q13, q23);
 }
 
 // hh_weno5M: OCFD_Schemes_1.f90:31-52 (OCFD_weno5M, OCFD_Schemes.f90:30-53)
@@ -50,14 +95,10 @@ __device__ __forceinline__ R weno5M(const R* v) {
   R S0 = k1312 * sq(v[1] - R(2) * v[0] + v[-1]) + k14 * sq(R(3) * v[1] - R(4) * v[0] + v[-1]);
   R S1 = k1312 * sq(v[2] - R(2) * v[1] + v[0]) + k14 * sq(v[2] - v[0]);
   R S2 = k1312 * sq(v[3] - R(2) * v[2] + v[1]) + k14 * sq(v[3] - R(4) * v[2] + R(3) * v[1]);
-  R a0 = C03 / sq(ep + S0);
-  R a1 = C13 / sq(ep + S1);
-  R a2 = C23 / sq(ep + S2);
-  R am = a0 + a1 + a2;
   R q03 = R(1.0 / 3.0) * v[1] + R(5.0 / 6.0) * v[0] - R(1.0 / 6.0) * v[-1];
   R q13 = R(-1.0 / 6.0) * v[2] + R(5.0 / 6.0) * v[1] + R(1.0 / 3.0) * v[0];
   R q23 = R(1.0 / 3.0) * v[3] - R(7.0 / 6.0) * v[2] + R(11.0 / 6.0) * v[1];
-  return (a0 * q03 + a1 * q13 + a2 * q23) / am;
+  return weno_sum3(ep, C03, C13, C23, S0, S1, S2, q03, q13, q23);
 }
 
 // hh_weno5P_boundary / hh_weno5M_boundary: OCFD_Schemes_1.f90:266-325.
@@ -142,16 +183,11 @@ __device__ __forceinline__ R weno7P(const R* v) {
   R S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
   R S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
   R S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
-  R a0 = C0 / sq(ep + S0);
-  R a1 = C1 / sq(ep + S1);
-  R a2 = C2 / sq(ep + S2);
-  R a3 = C3 / sq(ep + S3);
-  R am = a0 + a1 + a2 + a3;
   R q0 = e11 * v[-3] + e12 * v[-2] + e13 * v[-1] + e14 * v[0];
   R q1 = e21 * v[-2] + e22 * v[-1] + e23 * v[0] + e24 * v[1];
   R q2 = e31 * v[-1] + e32 * v[0] + e33 * v[1] + e34 * v[2];
   R q3 = e41 * v[0] + e42 * v[1] + e43 * v[2] + e44 * v[3];
-  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / am;
+  return weno_sum4(ep, C0, C1, C2, C3, S0, S1, S2, S3, q0, q1, q2, q3);
 }
 
 // hh_weno7M: OCFD_Schemes_1.f90:124-187 (OCFD_weno7M, OCFD_Schemes.f90:127-193)
@@ -174,16 +210,11 @@ __device__ __forceinline__ R weno7M(const R* v) {
   R S1 = S11 * S11 + d12 * S21 * S21 + d13 * S31 * S31 + d14 * S11 * S31;
   R S2 = S12 * S12 + d12 * S22 * S22 + d13 * S32 * S32 + d14 * S12 * S32;
   R S3 = S13 * S13 + d12 * S23 * S23 + d13 * S33 * S33 + d14 * S13 * S33;
-  R a0 = C0 / sq(ep + S0);
-  R a1 = C1 / sq(ep + S1);
-  R a2 = C2 / sq(ep + S2);
-  R a3 = C3 / sq(ep + S3);
-  R am = a0 + a1 + a2 + a3;
   R q0 = e11 * v[4] + e12 * v[3] + e13 * v[2] + e14 * v[1];
   R q1 = e21 * v[3] + e22 * v[2] + e23 * v[1] + e24 * v[0];
   R q2 = e31 * v[2] + e32 * v[1] + e33 * v[0] + e34 * v[-1];
   R q3 = e41 * v[1] + e42 * v[0] + e43 * v[-1] + e44 * v[-2];
-  return (a0 * q0 + a1 * q1 + a2 * q2 + a3 * q3) / am;
+  return weno_sum4(ep, C0, C1, C2, C3, S0, S1, S2, S3, q0, q1, q2, q3);
 }
 
 // minmod2 / minmod4: OCFD_Schemes.f90:274-289

@@ -70,7 +70,7 @@ def make_params(workload: str, precision: str, n_override: int | None = None):
 def byte_model(p) -> dict:
     r = 4 if p.precision == 1 else 8  # face fluxes / Ev / FP32 copies of prims+metrics
     s = 4 if p.precision == 1 else 8  # prims + metric rows read by the face kernels
-    nface = 5 if p.if_scheme_character else 10
+    nface = 5  # characteristic form: projected fluxes; flux-vector form: h(F+) + h(F-) per face
     face = 8 * s + nface * r  # d,u,v,w,T + 3 metric rows in; faces out
     visc = 4 * s + 18 * s + 12 * r  # u,v,w,T + 18 metrics in; 12 Ev out
     # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out

@@ -260,7 +260,7 @@ size_t ocfd_gpu_footprint(const ocfd_params* p) {
   b += OCFD_N_METRICS * nh * 8 + nh * 8;     // metrics, Rhybrid
   if (mixed) b += 5 * nh * 4 + OCFD_N_METRICS * nh * 4;
   const size_t faces = (size_t)(n / p->nx * (p->nx + 1) + n / p->ny * (p->ny + 1) + n / p->nz * (p->nz + 1));
-  b += faces * (chr ? 5 : 10) * r;
+  b += faces * ((chr || OCFD_FV_SUMMED) ? 5 : 10) * r;
   if (p->if_viscous) b += 12 * n * r;
   b += 2 * nh * 8 + 4096 * 8;                // scratch
   return b + (64u << 20);
@@ -360,7 +360,7 @@ int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
   }
   for (int d = 0; d < 3; d++) {
     h->fs[d] = g.nfaces(d);
-    AL(h->hf[d], (size_t)h->fs[d] * (h->chr ? 5 : 10) * r);
+    AL(h->hf[d], (size_t)h->fs[d] * ((h->chr || OCFD_FV_SUMMED) ? 5 : 10) * r);
   }
   if (p.if_viscous) AL(h->ev, 12 * n * r);
   h->scratch_n = std::max(rhybrid_scratch_doubles(g), std::max(2 * nh, reduce_scratch_doubles(g)));

@@ -76,6 +76,11 @@ struct Phys {
 #else
 #define OCFD_FEWER_DIVS 1
 #endif
+// Production build, flux-vector form: a face stores h(F+) + h(F-) (5 arrays)
+// instead of both terms (10 arrays), and the update kernel differences the
+// sums; the reference's order (h1(i) - h1(i-1) + h2(i) - h2(i-1)) is kept by
+// the strict build.
+#define OCFD_FV_SUMMED OCFD_FEWER_DIVS
 
 // Steger-Warming splitting of one point: split_Stager_Warming,
 // OCFD_flux_split.f90:5-70 (the P2 term is dropped there, :51-60).

@@ -352,8 +352,12 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #pragma unroll
           for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
           const R h2 = schemeM<SCHEME>(wv + 3, U, ihy);
-          out[fo + (long long)m * a.fs] = h1;
-          out[fo + (long long)(5 + m) * a.fs] = h2;
+          if (OCFD_FV_SUMMED) {
+            out[fo + (long long)m * a.fs] = h1 + h2;
+          } else {
+            out[fo + (long long)m * a.fs] = h1;
+            out[fo + (long long)(5 + m) * a.fs] = h2;
+          }
         }
       } else if (!ALLIN) {
 #pragma unroll 1
@@ -365,8 +369,12 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #pragma unroll
           for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
           const R h2 = nc_flux2_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
-          out[fo + (long long)m * a.fs] = h1;
-          out[fo + (long long)(5 + m) * a.fs] = h2;
+          if (OCFD_FV_SUMMED) {
+            out[fo + (long long)m * a.fs] = h1 + h2;
+          } else {
+            out[fo + (long long)m * a.fs] = h1;
+            out[fo + (long long)(5 + m) * a.fs] = h2;
+          }
         }
       }
       continue;

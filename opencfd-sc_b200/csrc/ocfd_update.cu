@@ -189,7 +189,7 @@ __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k
     for (int d = 0; d < 3; d++) {
       const R* H = a.hf[d];
       const long long fs = a.fs[d];
-      if (!CHAR)
+      if (!CHAR && !OCFD_FV_SUMMED)
         dd[d] = (H[f1[d] + m * fs] - H[f0[d] + m * fs] + H[f1[d] + (5 + m) * fs] - H[f0[d] + (5 + m) * fs]) *
                 R(a.h_1[d]);
       else

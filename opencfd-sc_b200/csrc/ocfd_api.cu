@@ -115,6 +115,7 @@ void fill_phys(const ocfd_params& p, Phys& ph, DCoef& dc) {
   ph.inv_g = 1.0 / p.gamma;
   ph.inv_gm1 = 1.0 / (p.gamma - 1.0);
   ph.sw_tmp3 = (3.0 - p.gamma) / (2.0 * (p.gamma - 1.0));
+  ph.inv_cv = 1.0 / p.cv;
   // OCFD_dxyz_viscous.f90:9-16
   const double hh[3] = {p.hx, p.hy, p.hz};
   for (int d = 0; d < 3; d++) {

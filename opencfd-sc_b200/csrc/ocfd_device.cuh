@@ -65,6 +65,7 @@ struct Phys {
   double inv_g;     // 1/gamma
   double inv_gm1;   // 1/(gamma-1)
   double sw_tmp3;   // (3-gamma)/(2(gamma-1))
+  double inv_cv;    // 1/Cv
 };
 
 // The production build replaces divisions by multiplications with a shared or

@@ -222,6 +222,11 @@ __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int 
   const int lc[3] = {i, j, k};
   const long long is[3] = {1, (long long)G.nx, (long long)G.nx * G.ny};
   const R ajac = R(a.ajac[G.ih(i, j, k)]);
+  // points within 4 of a periodic end read wrapped neighbours (the Ev arrays
+  // carry no halo); the others address their neighbours directly
+  bool wz[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) wz[d] = a.ph.periodic[d] && (lc[d] <= 4 || lc[d] > G.len(d) - 4);
 #pragma unroll
   for (int m = 0; m < 4; m++) {
     R s[3];
@@ -231,25 +236,39 @@ __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int 
       const int l = lc[d], nn = G.len(d);
       const int per = a.ph.periodic[d];
       const long long st = is[d];
-      auto at = [&](int off) -> R {
-        int l2 = l + off;
-        if (per) l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
-        return __ldg(E + (long long)(l2 - l) * st);
-      };
-      s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
+      if (!wz[d]) {
+        auto at = [&](int off) -> R { return __ldg(E + (long long)off * st); };
+        s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
+      } else {
+        auto at = [&](int off) -> R {
+          int l2 = l + off;
+          l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
+          return __ldg(E + (long long)(l2 - l) * st);
+        };
+        s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
+      }
     }
     du[m + 1] = du[m + 1] + (s[0] + s[1] + s[2]) * ajac;
   }
 }
 
 // primitive recovery of one point (comput_duvwT, OCFD_Time_Adv.f90:48-52)
-__device__ __forceinline__ void prims_of(const double* f, double cv, double* q) {
+// (production build: one reciprocal of the density instead of four divisions)
+__device__ __forceinline__ void prims_of(const double* f, double cv, double inv_cv, double* q) {
   const double f1 = f[0], f2 = f[1], f3 = f[2], f4 = f[3], f5 = f[4];
   q[0] = f1;
+#if OCFD_FEWER_DIVS
+  const double r1 = 1.0 / f1;
+  q[1] = f2 * r1;
+  q[2] = f3 * r1;
+  q[3] = f4 * r1;
+  q[4] = (f5 - (f2 * q[1] + f3 * q[2] + f4 * q[3]) * 0.5) * (r1 * inv_cv);
+#else
   q[1] = f2 / f1;
   q[2] = f3 / f1;
   q[3] = f4 / f1;
   q[4] = (f5 - (f2 * q[1] + f3 * q[2] + f4 * q[3]) * 0.5) / (f1 * cv);
+#endif
 }
 
 // f from primitives on a boundary face (OCFD_BC.f90:153-157)
@@ -364,7 +383,7 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
     for (int m = 0; m < 5; m++) fv[m] = al * a.fn[o + m * n] + be * (a.f[o + m * n] + dt * dd[m]);
   }
   double q[5];
-  prims_of(fv, a.ph.cv, q);
+  prims_of(fv, a.ph.cv, a.ph.inv_cv, q);
   const long long h = G.ih(i, j, k);
   if (q[4] <= 0.0) record_negt(a.st, h);
   if (FUSEBC && on_boundary_face(G, i, j, k)) refresh_of(q, a.ph.cv, fv);
@@ -479,7 +498,7 @@ __global__ void __launch_bounds__(256) k_duvwt(UpdArgs<double> a) {
   double fv[5], q[5];
 #pragma unroll
   for (int m = 0; m < 5; m++) fv[m] = a.f[o + m * n];
-  prims_of(fv, a.ph.cv, q);
+  prims_of(fv, a.ph.cv, a.ph.inv_cv, q);
   const long long h = G.ih(i, j, k);
   if (q[4] <= 0.0) record_negt(a.st, h);
 #pragma unroll

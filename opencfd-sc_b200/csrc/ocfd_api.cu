@@ -57,6 +57,7 @@ struct ocfd_handle {
   int ngraphs = 0;
   bool halo_valid = false;
   bool metrics_ready = false;
+  int met_version = 0;  // bumped whenever the metrics (and Phys::metzero) change
   int istep = 0;
   double tt = 0.0;
   std::string err;
@@ -408,6 +409,27 @@ static int refresh_p32(ocfd_handle* h) {
   return OCFD_OK;
 }
 
+// Records which metric arrays hold only +0.0 where the kernels read them
+// (Phys::metzero) and drops the captured step graphs, whose kernels carry the
+// previous value.
+static int refresh_metzero(ocfd_handle* h) {
+  unsigned int* d = reinterpret_cast<unsigned int*>(h->dout);
+  CK(launch_metric_nonzero(h->g, h->met, d, h->st));
+  CK(cudaMemcpyAsync(h->hout, d, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  unsigned int nz = 0;
+  memcpy(&nz, h->hout, sizeof(nz));
+  unsigned int cand = 0;
+  for (int m = 3; m < 22; m++)
+    if (m != OCFD_M_AJAC) cand |= 1u << m;
+  h->ph.metzero = cand & ~nz;
+  for (int q = 0; q < h->ngraphs; q++)
+    if (h->graphs[q].g) cudaGraphExecDestroy(h->graphs[q].g);
+  h->ngraphs = 0;
+  h->met_version++;
+  return OCFD_OK;
+}
+
 int ocfd_gpu_upload_metrics(ocfd_handle* h, const double* const metrics[OCFD_N_METRICS]) {
   if (!h || !metrics) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));
@@ -415,7 +437,8 @@ int ocfd_gpu_upload_metrics(ocfd_handle* h, const double* const metrics[OCFD_N_M
     if (metrics[m]) CK(cudaMemcpyAsync(h->met[m], metrics[m], h->g.nh * 8, cudaMemcpyHostToDevice, h->st));
   int r = refresh_met32(h);
   if (r) return r;
-  CK(cudaStreamSynchronize(h->st));
+  r = refresh_metzero(h);
+  if (r) return r;
   h->metrics_ready = true;
   return OCFD_OK;
 }
@@ -438,7 +461,8 @@ int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const d
   CK(launch_mesh(g, h->ph, h->dc, h->met, h->p.periodic_span, h->st));
   int r = refresh_met32(h);
   if (r) return r;
-  CK(cudaStreamSynchronize(h->st));
+  r = refresh_metzero(h);
+  if (r) return r;
   h->metrics_ready = true;
   return OCFD_OK;
 }
@@ -1031,6 +1055,7 @@ struct ocfd_batch {
     cudaGraphExec_t graph = nullptr;
   } par[2];
   std::vector<double*> f0, t0;  // members' f and T at table build (parity 0)
+  std::vector<int> mver;        // members' metric versions at table build
   int nblk_face[3] = {0, 0, 0}, nblk_upd = 0;
   std::string err;
 };
@@ -1320,9 +1345,11 @@ static int batch_prepare(ocfd_batch* b) {
   if (r) return r;
   b->f0.clear();
   b->t0.clear();
+  b->mver.clear();
   for (ocfd_handle* h : b->m) {
     b->f0.push_back(h->f);
     b->t0.push_back(h->prim[4]);
+    b->mver.push_back(h->met_version);
   }
   return OCFD_OK;
 }
@@ -1409,7 +1436,8 @@ int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
     bool ok = b->f0.size() == (size_t)n;
     for (int q = 0; q < n && ok; q++) {
       ocfd_handle* h = b->m[q];
-      const int pq = (h->f == b->f0[q] && h->prim[4] == b->t0[q]) ? 0 : (h->fn == b->f0[q] && h->talt == b->t0[q]) ? 1 : -1;
+      int pq = (h->f == b->f0[q] && h->prim[4] == b->t0[q]) ? 0 : (h->fn == b->f0[q] && h->talt == b->t0[q]) ? 1 : -1;
+      if (h->met_version != b->mver[q]) pq = -1;  // metrics changed: tables carry the old Phys
       if (pq < 0 || (par >= 0 && pq != par)) ok = false;
       par = pq;
     }

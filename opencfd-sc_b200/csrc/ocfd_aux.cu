@@ -395,6 +395,35 @@ cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* 
   return cudaGetLastError();
 }
 
+// Which metric arrays are +0.0 (all bits zero) at every point a kernel reads:
+// the interior and the face halos (edge and corner halos are never read).  On
+// box and 1-D grids the off-diagonal metrics are exact zeros; the face and
+// viscous kernels then skip their loads and use the constant (same bits).
+// Bit m of *nonzero is set when array m has a nonzero bit pattern there.
+__global__ void k_metric_nonzero(Grid G, MetPtrs mp, unsigned int* nonzero) {
+  unsigned int mask = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.nh;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nxh) - (LAP - 1), j = (int)((t / G.nxh) % G.nyh) - (LAP - 1);
+    const int k = (int)(t / ((long long)G.nxh * G.nyh)) - (LAP - 1);
+    const int out = (i < 1 || i > G.nx) + (j < 1 || j > G.ny) + (k < 1 || k > G.nz);
+    if (out > 1) continue;
+    for (int m = 3; m < 22; m++)
+      if (__double_as_longlong(mp.m[m][t]) != 0) mask |= 1u << m;
+  }
+  mask = __reduce_or_sync(0xffffffffu, mask);
+  if ((threadIdx.x & 31) == 0 && mask) atomicOr(nonzero, mask);
+}
+
+cudaError_t launch_metric_nonzero(const Grid& g, double* const met[22], unsigned int* nonzero, cudaStream_t st) {
+  MetPtrs mp;
+  for (int m = 0; m < 22; m++) mp.m[m] = met[m];
+  cudaError_t e = cudaMemsetAsync(nonzero, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  k_metric_nonzero<<<148 * 8, 256, 0, st>>>(g, mp, nonzero);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // filtering (OCFD_filtering.f90:4-363), one filter column
 __global__ void k_filt_copy(Grid G, int dir, int periodic, const double* src, double* f0) {

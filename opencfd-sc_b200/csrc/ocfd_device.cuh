@@ -66,6 +66,9 @@ struct Phys {
   double inv_gm1;   // 1/(gamma-1)
   double sw_tmp3;   // (3-gamma)/(2(gamma-1))
   double inv_cv;    // 1/Cv
+  // bit m: metric array m is +0.0 wherever the kernels read it (box grids:
+  // the off-diagonal metrics); its loads are skipped
+  unsigned int metzero;
 };
 
 // The production build replaces divisions by multiplications with a shared or
@@ -82,6 +85,12 @@ struct Phys {
 // sums; the reference's order (h1(i) - h1(i-1) + h2(i) - h2(i-1)) is kept by
 // the strict build.
 #define OCFD_FV_SUMMED OCFD_FEWER_DIVS
+
+// Metric m at haloed index c, or the constant +0.0 when the array holds only zeros.
+template <typename R, typename S>
+__device__ __forceinline__ R met_at(const Phys& ph, int m, const S* arr, long long c) {
+  return ((ph.metzero >> m) & 1u) ? R(0) : R(__ldg(arr + c));
+}
 
 // Steger-Warming splitting of one point: split_Stager_Warming,
 // OCFD_flux_split.f90:5-70 (the P2 term is dropped there, :51-60).

@@ -272,9 +272,9 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       v = R(__ldg(a.v + h));
       w = R(__ldg(a.w + h));
       T = R(__ldg(a.T + h));
-      A1 = R(__ldg(a.A1 + h));
-      A2 = R(__ldg(a.A2 + h));
-      A3 = R(__ldg(a.A3 + h));
+      A1 = met_at<R>(ph, 13 + 3 * DIR, a.A1, h);
+      A2 = met_at<R>(ph, 14 + 3 * DIR, a.A2, h);
+      A3 = met_at<R>(ph, 15 + 3 * DIR, a.A3, h);
     }
 #if OCFD_FEWER_DIVS
     const R c = sqrt(T) * R(ph.inv_ma);

@@ -177,6 +177,7 @@ cudaError_t launch_filter(const Grid& g, const Phys& ph, double* f, double* scra
                           cudaStream_t st);
 
 // init_mesh on the device: coords (3 haloed arrays, interior filled) -> metrics
+cudaError_t launch_metric_nonzero(const Grid& g, double* const met[22], unsigned int* nonzero, cudaStream_t st);
 cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* const met[22],
                         const double periodic_span[3][3], cudaStream_t st);
 

@@ -93,7 +93,7 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
     }
   R M[22];
 #pragma unroll
-  for (int m = 3; m < 22; m++) M[m] = R(__ldg(a.met[m] + c));
+  for (int m = 3; m < 22; m++) M[m] = met_at<R>(a.ph, m, a.met[m], c);
   const R Akx = M[3], Aky = M[4], Akz = M[5], Aix = M[6], Aiy = M[7], Aiz = M[8], Asx = M[9], Asy = M[10],
           Asz = M[11];
   const R ux = gr[0][0] * Akx + gr[0][1] * Aix + gr[0][2] * Asx;

@@ -67,15 +67,18 @@ def make_params(workload: str, precision: str, n_override: int | None = None):
 
 # ---------------------------------------------------------------------------------------------
 # byte model (algorithmic bytes per grid point, per launch) of each kernel group
-def byte_model(p) -> dict:
+def byte_model(p, zero_mask: int = 0) -> dict:
+    """Algorithmic bytes per grid point of each kernel launch.  zero_mask: the
+    metric arrays the library found identically zero (their loads are skipped)."""
     r = 4 if p.precision == 1 else 8  # face fluxes / Ev / FP32 copies of prims+metrics
     s = 4 if p.precision == 1 else 8  # prims + metric rows read by the face kernels
+    nz = lambda ms: sum(1 for m in ms if not (zero_mask >> m) & 1)
     nface = 5  # characteristic form: projected fluxes; flux-vector form: h(F+) + h(F-) per face
-    face = 8 * s + nface * r  # d,u,v,w,T + 3 metric rows in; faces out
-    visc = 4 * s + 18 * s + 12 * r  # u,v,w,T + 18 metrics in; 12 Ev out
+    face = {d: 5 * s + nz(range(13 + 3 * i, 16 + 3 * i)) * s + nface * r for i, d in enumerate(("x", "y", "z"))}
+    visc = 4 * s + nz(range(3, 22)) * s + 12 * r  # u,v,w,T + non-zero metrics in; 12 Ev out
     # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out
     tail = 3 * nface * r + 12 * r + 8 + 40 + 40 * 2.0 / 3.0 + 40 + 40 + (20 if p.precision == 1 else 0)
-    return {"face_x": face, "face_y": face, "face_z": face, "visc_grad": visc, "stage_tail": tail}
+    return {"face_x": face["x"], "face_y": face["y"], "face_z": face["z"], "visc_grad": visc, "stage_tail": tail}
 
 
 def load_peaks():
@@ -259,7 +262,7 @@ def run_ours(args):
 
     # ---- per-kernel timing (roofline of the dominant kernel)
     prof = s.profile_steps(3)
-    model = byte_model(s.p)
+    model = byte_model(s.p, s.metric_zero_mask())
     groups = {k: v for k, v in prof.items() if k in model}
     dom = max(groups, key=groups.get)
     t_launch = groups[dom] / 3.0 * 1e-3  # 3 launches per step
@@ -329,7 +332,10 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "bytes_per_point": model[dom],
-                         "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()}},
+                         "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+                         "note": ("the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM "
+                                  "bound: ncu pipe and DRAM fractions per kernel in "
+                                  "profiles/kernels_tgv128_omp6_char.md")},
             "cpu_baseline": cpu,
             "kinetic_energy": ke,
         }
@@ -407,6 +413,55 @@ def run_serve(args):
     return 0
 
 
+def run_history(args):
+    """Kinetic-energy, dissipation-rate (-dK/dt) and enstrophy histories of the
+    256^3 characteristic TGV runs (OMP6 and hybrid): the GPU production build
+    against the oracle over the first `--hist-oracle-steps` steps (the oracle
+    needs seconds per step at this size), and the GPU alone over the full
+    `--hist-steps` steps."""
+    import numpy as np
+
+    from ocfd_b200.solver import Solver
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle
+
+    from ocfd_b200 import cases
+
+    every = args.hist_every
+    out = {"mode": "history", "grid": "256^3", "dt": WORKLOADS["tgv256_omp6_char"][4], "every": every,
+           "data": "synthetic (analytic Taylor-Green initial field)"}
+    for wl in ("tgv256_omp6_char", "tgv256_hybrid_char"):
+        rec = {}
+        for kind in ("gpu", "oracle"):
+            p = make_params(wl, "fp64")
+            steps = args.hist_steps if kind == "gpu" else args.hist_oracle_steps
+            s = Solver(p) if kind == "gpu" else Oracle(p)
+            s.init_mesh()
+            s.init3d(cases.tgv_prims(s.p))
+            t, ke, ens = [0.0], [float(s.show_flow_msg()[1])], [float(s.ana_box()[13])]
+            done = 0
+            while done < steps:
+                k = min(every, steps - done)
+                s.step(k)
+                done += k
+                t.append(done * p.dt)
+                ke.append(float(s.show_flow_msg()[1]))
+                ens.append(float(s.ana_box()[13]))
+            s.close()
+            t, ke = np.array(t), np.array(ke)
+            eps = -(ke[1:] - ke[:-1]) / (t[1:] - t[:-1])
+            rec[kind] = {"t": t.tolist(), "ke": ke.tolist(), "eps": eps.tolist(), "enstrophy": ens}
+        g, o = rec["gpu"], rec["oracle"]
+        m = len(o["ke"])
+        rel = lambda a, b: float(np.max(np.abs(np.array(a) - np.array(b)) / np.maximum(np.abs(np.array(b)), 1e-300)))
+        out[wl] = {"gpu_steps": args.hist_steps, "oracle_steps": args.hist_oracle_steps,
+                   "ke_rel_max": rel(g["ke"][:m], o["ke"]), "eps_rel_max": rel(g["eps"][:m - 1], o["eps"]),
+                   "enstrophy_rel_max": rel(g["enstrophy"][:m], o["enstrophy"]), "gpu": g, "oracle": o}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -420,6 +475,10 @@ def main():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--round-steps", type=int, default=25)
+    ap.add_argument("--history", action="store_true", help="kinetic-energy / dissipation histories vs the oracle")
+    ap.add_argument("--hist-steps", type=int, default=500)
+    ap.add_argument("--hist-oracle-steps", type=int, default=20)
+    ap.add_argument("--hist-every", type=int, default=5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -427,6 +486,8 @@ def main():
         return run_reference(args)
     if args.serve:
         return run_serve(args)
+    if args.history:
+        return run_history(args)
     return run_ours(args)
 
 

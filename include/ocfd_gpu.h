@@ -185,6 +185,13 @@ int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const d
 /* Download the 22 haloed metric arrays (for checks and for the host's analysis). */
 int ocfd_gpu_download_metrics(ocfd_handle* h, double* const metrics[OCFD_N_METRICS]);
 
+/* Bit m set: metric array m (OCFD_M_*) holds +0.0 at every point the kernels
+ * read (interior and face halos), so its loads are skipped -- the off-diagonal
+ * metrics of box and 1-D grids.  Known after init_mesh / upload_metrics.  No
+ * counterpart in the reference (an internal optimisation made visible for
+ * tests and byte accounting). */
+unsigned int ocfd_gpu_metric_zero_mask(const ocfd_handle* h);
+
 /* ---------------------------------------------------------------------------
  * State transfer (sync points of NS_solver: init3d, show, analysis, save)
  * ------------------------------------------------------------------------- */

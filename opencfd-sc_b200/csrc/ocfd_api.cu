@@ -467,6 +467,8 @@ int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const d
   return OCFD_OK;
 }
 
+unsigned int ocfd_gpu_metric_zero_mask(const ocfd_handle* h) { return h ? h->ph.metzero : 0u; }
+
 int ocfd_gpu_download_metrics(ocfd_handle* h, double* const metrics[OCFD_N_METRICS]) {
   if (!h) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));

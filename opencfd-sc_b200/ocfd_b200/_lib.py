@@ -95,6 +95,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_batch_step.restype = C.c_int
     L.ocfd_batch_destroy.argtypes = [H]
     L.ocfd_batch_destroy.restype = None
+    L.ocfd_gpu_metric_zero_mask.argtypes = [H]
+    L.ocfd_gpu_metric_zero_mask.restype = C.c_uint
     L.ocfd_batch_set_tiles.argtypes = [H, C.POINTER(C.c_int)]
     L.ocfd_batch_set_tiles.restype = C.c_int
     L.ocfd_batch_info.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -127,5 +129,5 @@ EXPORTED = [
     "ocfd_gpu_du_viscous", "ocfd_gpu_rk3", "ocfd_gpu_duvwt", "ocfd_gpu_bc", "ocfd_gpu_filter",
     "ocfd_gpu_advance_clock", "ocfd_gpu_step", "ocfd_gpu_show_flow_msg", "ocfd_gpu_ana_box", "ocfd_batch_create",
     "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps", "ocfd_show_flow_msg_noalloc",
-    "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error",
+    "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error", "ocfd_gpu_metric_zero_mask",
 ]

@@ -96,6 +96,10 @@ class Solver:
         arr = (C.POINTER(C.c_double) * 22)(*[_dp(m) for m in ms])
         self._check(self.L.ocfd_gpu_upload_metrics(self.h, arr), "upload_metrics")
 
+    def metric_zero_mask(self) -> int:
+        """Bit m: metric m is identically +0.0 where the kernels read it (loads skipped)."""
+        return int(self.L.ocfd_gpu_metric_zero_mask(self.h))
+
     def download_metrics(self):
         ms = [np.empty(self.shape_h) for _ in range(N_METRICS)]
         arr = (C.POINTER(C.c_double) * 22)(*[_dp(m) for m in ms])

@@ -240,3 +240,24 @@ def test_mixed_precision_close_to_fp64():
     assert rel_l2(fb, fa) < 1e-6
     ea, eb = a.show_flow_msg(), b.show_flow_msg()
     assert abs(eb[1] - ea[1]) / ea[1] < 1e-6
+
+
+def test_metric_zero_mask_box_and_curvilinear():
+    """Box grids: exactly the twelve off-diagonal metric arrays are +0.0 where the
+    kernels read them (their loads are skipped); on a body-fitted grid the
+    in-plane metrics are not."""
+    from ocfd_b200.solver import Solver
+
+    p, _, prims = tgv_case()
+    s = Solver(p)
+    s.init_mesh()
+    off = [4, 5, 6, 8, 9, 10, 14, 15, 16, 18, 19, 20]
+    assert s.metric_zero_mask() == sum(1 << m for m in off)
+    s.close()
+    p, X, prims = curvilinear_case()
+    s = Solver(p)
+    s.init_mesh(*X)
+    # the in-plane metrics of the body-fitted grid are never flagged
+    for m in (3, 4, 6, 7, 11, 13, 14, 16, 17, 21):
+        assert not (s.metric_zero_mask() >> m) & 1, m
+    s.close()

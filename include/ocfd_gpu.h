@@ -146,8 +146,9 @@ void ocfd_default_params(ocfd_params* p);
 
 /* set_parameters + set_scheme_para (OCFD_readpara.f90:261-341) for one rank
  * owning the whole grid.  Validates the configuration; returns OCFD_E_PARAM for
- * anything this library does not implement (BC_BoundaryLayer, BC_SweptCorner,
- * SCHEME_USER, LAP != 4, grids smaller than the stencils). */
+ * anything this library does not implement (SCHEME_USER, LAP != 4, grids
+ * smaller than the stencils, BC_BoundaryLayer / BC_SweptCorner with a periodic
+ * x or y direction). */
 int ocfd_set_parameters(ocfd_params* p);
 
 /* Bytes of device memory an instance with these parameters needs (admission). */
@@ -237,8 +238,37 @@ int ocfd_gpu_rk3(ocfd_handle* h, int krk);
  * of repaired points; returns OCFD_E_NEGT when it exceeds 10. */
 int ocfd_gpu_duvwt(ocfd_handle* h, int* num_negt);
 /* OCFD_bc (OCFD_BC.f90:2-99): BC dispatch, f refresh on the six faces,
- * Flow_Ghost_boundary (OCFD_GhostCell.f90:9-14,164-286). */
+ * Flow_Ghost_boundary (OCFD_GhostCell.f90:9-14,164-286, user ghost cells
+ * OCFD_GhostCell_UserDef.f90:13-20). */
 int ocfd_gpu_bc(ocfd_handle* h);
+
+/* Boundary data of BC_BoundaryLayer (ocfd_bc_BoundaryLayer,
+ * OCFD_BC_Boundarylayers.f90:17-169) and BC_SweptCorner (ocfd_bc_swept_corner,
+ * :443-618), which the reference builds at its first BC call:
+ * init_bcdata_boundarylayer (:171-270) reads flow1d/flow2d-inlet.dat and
+ * -upper.dat, init_bc_wall_perturbation (:313-400) and get_ht_multifrequancy
+ * (:404-440) draw random phases.  The host passes the results; the library
+ * computes init_bc_nonRef (:273-311) from the mesh.  Arrays in Fortran order,
+ * NULL for zeros:
+ *   inlet (ny,nz,5)  d,u,v,w,T at i = 1 (used when BC_Para(1) != 0, and always
+ *                    by BC_SweptCorner)
+ *   upper (nx,nz,5)  at j = ny (used when BC_Para(2) != 0)
+ *   pertb (nx,nz)    wall blowing/suction shape wall_pertb
+ *   mt, beta, tm, fait: time factor ht = sum_m tm[m-1] sin(m beta tt + 2 pi fait[m-1])
+ *                    (beta <= 0: ht = 1)
+ * Call after the mesh is set.  With the free-stream inlet and upper boundary
+ * and no perturbation it may be omitted (the first BC call sets the mask).
+ * A wall perturbation that varies in time disables the captured step graphs. */
+typedef struct ocfd_bc_layer {
+  const double* inlet;
+  const double* upper;
+  const double* pertb;
+  int32_t mt;
+  double beta;
+  const double* tm;
+  const double* fait;
+} ocfd_bc_layer;
+int ocfd_gpu_set_bc_layer(ocfd_handle* h, const ocfd_bc_layer* d);
 /* filtering(f) (OCFD_filtering.f90:4-70) for the current Istep. */
 int ocfd_gpu_filter(ocfd_handle* h);
 /* Istep += 1, tt += dt (OCFD_NS_Solver.f90:64-65). */

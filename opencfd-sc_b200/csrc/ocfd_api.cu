@@ -58,6 +58,15 @@ struct ocfd_handle {
   bool halo_valid = false;
   bool metrics_ready = false;
   int met_version = 0;  // bumped whenever the metrics (and Phys::metzero) change
+  // BC_BoundaryLayer / BC_SweptCorner boundary data (device) and time factor (host)
+  double* bl_inlet = nullptr;
+  double* bl_upper = nullptr;
+  double* bl_pertb = nullptr;
+  int* bl_mask = nullptr;
+  bool bl_ready = false;
+  bool bl_time_dep = false;  // the wall condition changes with tt: no captured step graphs
+  double bl_beta = 0.0;
+  std::vector<double> bl_tm, bl_fait;
   int istep = 0;
   double tt = 0.0;
   std::string err;
@@ -111,6 +120,7 @@ void fill_phys(const ocfd_params& p, Phys& ph, DCoef& dc) {
   ph.kb2 = p.kb2;
   ph.ibc = p.ibc;
   ph.bc_para0 = p.bc_para[0];
+  for (int q = 0; q < 14; q++) ph.bc_p[q] = p.bc_para[q];
   ph.inv_ma = 1.0 / p.ma;
   ph.inv_2g = 1.0 / (2.0 * p.gamma);
   ph.inv_g = 1.0 / p.gamma;
@@ -212,11 +222,16 @@ int ocfd_set_parameters(ocfd_params* p) {
   }
   if (p->scheme_vis != OCFD_SCHEME_CD6 && p->scheme_vis != OCFD_SCHEME_CD8) return OCFD_E_PARAM;
   if (p->flux_splitting != OCFD_SPLIT_SW && p->flux_splitting != OCFD_SPLIT_LLF) return OCFD_E_PARAM;
-  if (p->ibc != OCFD_BC_NONE && p->ibc != OCFD_BC_BLUNT2D && p->ibc != OCFD_BC_USER_DEF) return OCFD_E_PARAM;
+  if (p->ibc != OCFD_BC_NONE && p->ibc != OCFD_BC_BLUNT2D && p->ibc != OCFD_BC_USER_DEF &&
+      p->ibc != OCFD_BC_BOUNDARYLAYER && p->ibc != OCFD_BC_SWEPTCORNER)
+    return OCFD_E_PARAM;
   if (p->ibc == OCFD_BC_USER_DEF && !(p->bc_para[0] > 0.0)) return OCFD_E_PARAM;
+  if ((p->ibc == OCFD_BC_BOUNDARYLAYER || p->ibc == OCFD_BC_SWEPTCORNER) && (p->iperiodic[0] || p->iperiodic[1]))
+    return OCFD_E_PARAM;  // inlet/outlet at i = 1/nx and wall/upper at j = 1/ny
   for (int q = 0; q < 6; q++) {
     if (p->scheme_boundary[q] < -1 || p->scheme_boundary[q] > 1) return OCFD_E_PARAM;
-    if (p->ghost_cell[q] < 0 || p->ghost_cell[q] > 2) return OCFD_E_PARAM;
+    // -1: user-defined ghost cells (flat-plate j- face, swept-corner k- face)
+    if (p->ghost_cell[q] < -1 || p->ghost_cell[q] > 2) return OCFD_E_PARAM;
   }
   if (p->nfiltering < 0 || p->nfiltering > 10) return OCFD_E_PARAM;
   if (p->precision != OCFD_PRECISION_FP64 && p->precision != OCFD_PRECISION_MIXED) return OCFD_E_PARAM;
@@ -309,6 +324,10 @@ void ocfd_gpu_destroy(ocfd_handle* h) {
   F(h->dstat);
   F(h->dout);
   F(h->dptr);
+  F(h->bl_inlet);
+  F(h->bl_upper);
+  F(h->bl_pertb);
+  F(h->bl_mask);
   if (h->hstat) cudaFreeHost(h->hstat);
   if (h->hout) cudaFreeHost(h->hout);
   if (h->st) cudaStreamDestroy(h->st);
@@ -775,10 +794,93 @@ int ocfd_gpu_duvwt(ocfd_handle* h, int* num_negt) {
   return OCFD_OK;
 }
 
+// get_ht_multifrequancy (OCFD_BC_Boundarylayers.f90:404-440) at the current tt
+static double bl_ht(const ocfd_handle* h) {
+  const double PI = 3.14159265358979;
+  if (!(h->bl_beta > 0.0)) return 1.0;
+  double ht = 0.0;
+  for (size_t m = 1; m <= h->bl_tm.size(); m++)
+    ht = ht + h->bl_tm[m - 1] * std::sin(m * h->bl_beta * h->tt + 2.0 * PI * h->bl_fait[m - 1]);
+  return ht;
+}
+
+// The BC of OCFD_bc (OCFD_BC.f90:8-24) for the instance's BoundaryCondition.
+static int bc_dispatch(ocfd_handle* h) {
+  if (h->p.ibc == OCFD_BC_BOUNDARYLAYER || h->p.ibc == OCFD_BC_SWEPTCORNER) {
+    if (!h->bl_ready) {
+      // the reference's first call builds its data; without host data only the
+      // free-stream inlet / upper boundary are available
+      const bool needs = h->p.ibc == OCFD_BC_SWEPTCORNER || std::llround(h->p.bc_para[0]) != 0 ||
+                         std::llround(h->p.bc_para[1]) != 0;
+      if (needs) return fail(h, OCFD_E_STATE, "boundary data not set (ocfd_gpu_set_bc_layer)");
+      int r = ocfd_gpu_set_bc_layer(h, nullptr);
+      if (r) return r;
+    }
+    BcLayer bl;
+    bl.inlet = h->bl_inlet;
+    bl.upper = h->bl_upper;
+    bl.pertb = h->bl_pertb;
+    bl.dirichlet = h->bl_mask;
+    bl.aix = h->met[OCFD_M_AIX];
+    bl.aiy = h->met[OCFD_M_AIY];
+    bl.aiz = h->met[OCFD_M_AIZ];
+    bl.ayy = h->met[OCFD_M_AYY];
+    bl.azz = h->met[OCFD_M_AZZ];
+    bl.ht = bl_ht(h);
+    bl.u0 = std::cos(h->p.aoa);
+    bl.v0 = std::sin(h->p.aoa);
+    CK(launch_bc_layer(h->g, h->ph, bl, h->prim, h->st));
+    return OCFD_OK;
+  }
+  CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_set_bc_layer(ocfd_handle* h, const ocfd_bc_layer* d) {
+  if (!h) return OCFD_E_PARAM;
+  if (h->p.ibc != OCFD_BC_BOUNDARYLAYER && h->p.ibc != OCFD_BC_SWEPTCORNER)
+    return fail(h, OCFD_E_STATE, "BoundaryCondition is not BC_BoundaryLayer or BC_SweptCorner");
+  if (!h->metrics_ready) return fail(h, OCFD_E_STATE, "set the mesh first (the upper-boundary mask reads it)");
+  if (d && d->mt > 0 && (!d->tm || !d->fait)) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  const Grid& g = h->g;
+  const size_t ni = (size_t)g.ny * g.nz * 5, nu = (size_t)g.nx * g.nz * 5, np = (size_t)g.nx * g.nz;
+  if (!h->bl_inlet) {
+    CK(cudaMalloc((void**)&h->bl_inlet, ni * 8));
+    CK(cudaMalloc((void**)&h->bl_upper, nu * 8));
+    CK(cudaMalloc((void**)&h->bl_pertb, np * 8));
+    CK(cudaMalloc((void**)&h->bl_mask, np * sizeof(int)));
+  }
+  CK(cudaMemsetAsync(h->bl_inlet, 0, ni * 8, h->st));
+  CK(cudaMemsetAsync(h->bl_upper, 0, nu * 8, h->st));
+  CK(cudaMemsetAsync(h->bl_pertb, 0, np * 8, h->st));
+  if (d && d->inlet) CK(cudaMemcpyAsync(h->bl_inlet, d->inlet, ni * 8, cudaMemcpyHostToDevice, h->st));
+  if (d && d->upper) CK(cudaMemcpyAsync(h->bl_upper, d->upper, nu * 8, cudaMemcpyHostToDevice, h->st));
+  bool pert = false;
+  if (d && d->pertb) {
+    CK(cudaMemcpyAsync(h->bl_pertb, d->pertb, np * 8, cudaMemcpyHostToDevice, h->st));
+    for (size_t c = 0; c < np && !pert; c++) pert = d->pertb[c] != 0.0;
+  }
+  const int mode = h->p.ibc == OCFD_BC_SWEPTCORNER ? 0 : (int)std::llround(h->p.bc_para[2]);
+  CK(launch_bc_layer_mask(g, h->met[OCFD_M_AXX], h->met[OCFD_M_AYY], mode, std::tan(h->p.aoa), h->bl_mask, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->bl_tm.assign(d && d->mt > 0 ? d->tm : nullptr, d && d->mt > 0 ? d->tm + d->mt : nullptr);
+  h->bl_fait.assign(d && d->mt > 0 ? d->fait : nullptr, d && d->mt > 0 ? d->fait + d->mt : nullptr);
+  h->bl_beta = d ? d->beta : 0.0;
+  const double A = h->p.ibc == OCFD_BC_SWEPTCORNER ? h->p.bc_para[4] : h->p.bc_para[7];
+  h->bl_time_dep = pert && A != 0.0 && h->bl_beta > 0.0;
+  h->bl_ready = true;
+  for (int q = 0; q < h->ngraphs; q++)
+    if (h->graphs[q].g) cudaGraphExecDestroy(h->graphs[q].g);
+  h->ngraphs = 0;
+  return OCFD_OK;
+}
+
 int ocfd_gpu_bc(ocfd_handle* h) {
   if (!h) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));
-  CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
+  int r = bc_dispatch(h);
+  if (r) return r;
   CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
   CK(launch_ghost(h->g, h->ph, h->prim, h->st));
   return refresh_p32(h);
@@ -855,7 +957,8 @@ static int fused_stage(ocfd_handle* h, int krk, Prof* pf = nullptr) {
   CK(launch_negt_fix(fx, h->st));
   swap_t(h);
   if (!h->fuse_bc) {
-    CK(launch_bc_wall(h->g, h->ph, h->prim, h->st));
+    int rb = bc_dispatch(h);
+    if (rb) return rb;
     CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
     CK(launch_ghost(h->g, h->ph, h->prim, h->st));
     int r = halo_all(h);
@@ -929,7 +1032,7 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
     if (r) return r;
     h->halo_valid = true;
   }
-  const bool use_graph = h->p.nfiltering == 0;
+  const bool use_graph = h->p.nfiltering == 0 && !h->bl_time_dep;
   for (int s = 0; s < nsteps; s++) {
     if (!use_graph) {
       int r = fused_step(h);

@@ -359,6 +359,36 @@ __global__ void k_jac_ghost_metrics(Grid G, Phys ph, int nb, MetPtrs mp) {
   }
 }
 
+// Jac_Ghost_Userdef (OCFD_GhostCell_UserDef.f90:4-11): mirrored metrics and
+// coordinates with the sign of the reflected components flipped -- swept corner
+// k- symmetry about z = 0 (Jac_Ghost_Sweptcorner :23-49), flat plate j-
+// symmetry about y = 0 (Jac_Ghost_flatplate :76-102).
+__global__ void k_jac_ghost_user(Grid G, Phys ph, MetPtrs mp) {
+  double* const* M = mp.m;
+  const bool sc = ph.ibc == 3 && ph.ghost[4] == -1;
+  // Akx Aky Akz Aix Aiy Aiz Asx Asy Asz Ajac (ids 3..12) and Axx Ayy Azz (0..2)
+  const int ids[13] = {3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 0, 1, 2};
+  const double sgz[13] = {1, 1, -1, 1, 1, -1, -1, -1, 1, 1, 1, 1, -1};
+  const double sgy[13] = {1, -1, 1, -1, 1, -1, 1, -1, 1, 1, 1, -1, 1};
+  const long long tot = sc ? (long long)G.nx * G.ny * LAP : (long long)G.nx * G.nz * LAP;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    long long h, h1;
+    if (sc) {
+      const int i = (int)(t % G.nx) + 1, j = (int)((t / G.nx) % G.ny) + 1, k = 1 - LAP + (int)(t / ((long long)G.nx * G.ny));
+      h = G.ih(i, j, k);
+      h1 = G.ih(i, j, 1 - k);
+    } else {
+      const int i = (int)(t % G.nx) + 1, k = (int)((t / G.nx) % G.nz) + 1, j = 1 - LAP + (int)(t / ((long long)G.nx * G.nz));
+      h = G.ih(i, j, k);
+      h1 = G.ih(i, 2 - j, k);
+    }
+    for (int q = 0; q < 13; q++) {
+      const double x = M[ids[q]][h1];
+      M[ids[q]][h] = (sc ? sgz[q] : sgy[q]) < 0 ? -x : x;
+    }
+  }
+}
+
 // Akx1 = Akx/Ajac ... over the whole haloed box (OCFD_mesh.f90:41-55)
 __global__ void k_metric_div(long long nh, MetPtrs mp) {
   double* const* M = mp.m;
@@ -391,6 +421,8 @@ cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* 
   k_jac_ghost_coords<<<148 * 2, 256, 0, st>>>(g, ph, 2, mp);
   for (int f = 0; f < 6; f++)
     if (ph.ghost[f] == 2) k_jac_ghost_metrics<<<148 * 2, 256, 0, st>>>(g, ph, f + 1, mp);
+  if ((ph.ibc == 3 && ph.ghost[4] == -1) || (ph.ibc == 2 && ph.ghost[2] == -1))
+    k_jac_ghost_user<<<148 * 2, 256, 0, st>>>(g, ph, mp);
   k_metric_div<<<148 * 8, 256, 0, st>>>(g.nh, mp);
   return cudaGetLastError();
 }

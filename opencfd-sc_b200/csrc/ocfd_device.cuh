@@ -59,6 +59,7 @@ struct Phys {
   int ibc;
   int ghost[6];
   double bc_para0;
+  double bc_p[14];  // BC_Para(1:14) of BC_BoundaryLayer / BC_SweptCorner
   // reciprocals precomputed on the host for the production build
   double inv_ma;    // 1/Ma
   double inv_2g;    // 1/(2 gamma)

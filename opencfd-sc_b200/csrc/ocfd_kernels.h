@@ -157,6 +157,25 @@ cudaError_t launch_halo(const Grid& g, const int periodic[3], PtrList<double> ar
 cudaError_t launch_halo_f32(const Grid& g, const int periodic[3], PtrList<float> arrs, cudaStream_t st);
 // BC dispatch on the primitives (blunt2d / user isothermal wall)
 cudaError_t launch_bc_wall(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
+// BC_BoundaryLayer / BC_SweptCorner (OCFD_BC_Boundarylayers.f90): boundary data
+// on the device and the per-call scalars.
+struct BcLayer {
+  const double* inlet;   // (ny,nz,5) at i = 1
+  const double* upper;   // (nx,nz,5) at j = ny
+  const double* pertb;   // (nx,nz) wall perturbation shape
+  const int* dirichlet;  // (nx,nz) 1: Dirichlet upper boundary, 0: non-reflecting
+  const double* aix;     // haloed metrics read by the wall condition
+  const double* aiy;
+  const double* aiz;
+  const double* ayy;     // haloed coordinates read by the swept-corner wall test
+  const double* azz;
+  double ht;             // wall perturbation time factor at this step's tt
+  double u0, v0;         // cos(AoA), sin(AoA)
+};
+cudaError_t launch_bc_layer(const Grid& g, const Phys& ph, const BcLayer& bl, double* const prim[5], cudaStream_t st);
+// init_bc_nonRef (OCFD_BC_Boundarylayers.f90:273-311): Dirichlet mask of the upper boundary
+cudaError_t launch_bc_layer_mask(const Grid& g, const double* axx, const double* ayy, int mode, double sy0, int* mask,
+                                 cudaStream_t st);
 // f refresh on the six faces from the primitives (OCFD_BC.f90:150-218)
 cudaError_t launch_bc_refresh(const Grid& g, const Phys& ph, double* f, double* const prim[5], cudaStream_t st);
 // Flow_Ghost_Extent_2nd

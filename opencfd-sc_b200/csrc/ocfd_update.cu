@@ -732,6 +732,182 @@ cudaError_t launch_bc_refresh(const Grid& g, const Phys& ph, double* f, double* 
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// BC_BoundaryLayer (ocfd_bc_BoundaryLayer, OCFD_BC_Boundarylayers.f90:17-169) and
+// BC_SweptCorner (ocfd_bc_swept_corner, :443-618).  The reference's loops run in
+// this order -- inlet, upper, wall, outlet (, side planes) -- and later loops
+// read points earlier ones wrote, so each is one launch.
+__global__ void k_bcl_inlet(Grid G, Phys ph, BcLayer bl, double* d, double* u, double* v, double* w, double* T) {
+  const long long tot = (long long)G.ny * G.nz, nyz = tot;
+  const int data = ph.ibc == 3 ? 1 : (int)llrint(ph.bc_p[0]);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(t % G.ny) + 1, k = (int)(t / G.ny) + 1;
+    const long long h = G.ih(1, j, k);
+    if (data == 0) {
+      // the reference's free-stream inlet sets T = 0 (:58-66)
+      d[h] = 1.0;
+      u[h] = bl.u0;
+      v[h] = bl.v0;
+      w[h] = 0.0;
+      T[h] = 0.0;
+    } else {
+      d[h] = bl.inlet[t];
+      u[h] = bl.inlet[t + nyz];
+      v[h] = bl.inlet[t + 2 * nyz];
+      w[h] = bl.inlet[t + 3 * nyz];
+      T[h] = bl.inlet[t + 4 * nyz];
+    }
+  }
+}
+__global__ void k_bcl_upper(Grid G, Phys ph, BcLayer bl, double* d, double* u, double* v, double* w, double* T) {
+  const long long tot = (long long)G.nx * G.nz, nxz = tot;
+  const int data = ph.ibc == 3 ? 0 : (int)llrint(ph.bc_p[1]);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    if (!bl.dirichlet[t]) continue;
+    const int i = (int)(t % G.nx) + 1, k = (int)(t / G.nx) + 1;
+    const long long h = G.ih(i, G.ny, k);
+    if (data == 0) {
+      d[h] = 1.0;
+      u[h] = bl.u0;
+      v[h] = bl.v0;
+      w[h] = 0.0;
+      T[h] = 1.0;
+    } else {
+      d[h] = bl.upper[t];
+      u[h] = bl.upper[t + nxz];
+      v[h] = bl.upper[t + 2 * nxz];
+      w[h] = bl.upper[t + 3 * nxz];
+      T[h] = bl.upper[t + 4 * nxz];
+    }
+  }
+}
+__global__ void k_bcl_wall(Grid G, Phys ph, BcLayer bl, double* d, double* u, double* v, double* w, double* T) {
+  const long long tot = (long long)G.nx * G.nz;
+  const bool sc = ph.ibc == 3;
+  const double Tw = sc ? ph.bc_p[1] : ph.bc_p[4];
+  const double A = sc ? ph.bc_p[4] : ph.bc_p[7];
+  const double wall_zl = ph.bc_p[2], epsl = 1.0e-7;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nx) + 1, k = (int)(t / G.nx) + 1;
+    const long long h1 = G.ih(i, 1, k), h2 = G.ih(i, 2, k), h3 = G.ih(i, 3, k);
+    if (sc) {
+      const double zz = bl.azz[h1], yy = bl.ayy[h1];
+      if (!((zz >= -epsl && zz <= wall_zl + epsl) || yy <= epsl)) {
+        // off the wall: first-order extrapolation (:552-558)
+        d[h1] = d[h2];
+        T[h1] = T[h2];
+        u[h1] = u[h2];
+        v[h1] = v[h2];
+        w[h1] = w[h2];
+        continue;
+      }
+    }
+    const double aix = bl.aix[h1], aiy = bl.aiy[h1], aiz = bl.aiz[h1];
+    const double tmp = 1.0 / (sqrt(aix * aix + aiy * aiy + aiz * aiz));
+    const double A0 = A * bl.ht * bl.pertb[t];
+    u[h1] = A0 * aix * tmp;
+    v[h1] = A0 * aiy * tmp;
+    w[h1] = A0 * aiz * tmp;
+    if (Tw > 0.0) {
+      T[h1] = Tw;
+      d[h1] = (4.0 * d[h2] * T[h2] - d[h3] * T[h3]) / (3.0 * Tw);
+    } else {
+      T[h1] = (4.0 * T[h2] - T[h3]) / 3.0;
+      d[h1] = (4.0 * d[h2] - d[h3]) / 3.0;
+    }
+  }
+}
+__global__ void k_bcl_outlet(Grid G, int mode, double* d, double* u, double* v, double* w, double* T) {
+  const long long tot = (long long)G.ny * G.nz;
+  double* Q[5] = {d, u, v, w, T};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(t % G.ny) + 1, k = (int)(t / G.ny) + 1;
+    const long long h = G.ih(G.nx, j, k), h1 = G.ih(G.nx - 1, j, k), h2 = G.ih(G.nx - 2, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; q++) Q[q][h] = mode == 1 ? Q[q][h1] : 2.0 * Q[q][h1] - Q[q][h2];
+  }
+}
+// swept corner side planes k = 1 (from k = 2) and k = nz (from nz - 1), :573-618
+__global__ void k_bcl_zside(Grid G, int kdst, int ksrc, double* d, double* u, double* v, double* w, double* T) {
+  const long long tot = (long long)G.nx * G.ny;
+  double* Q[5] = {d, u, v, w, T};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nx) + 1, j = (int)(t / G.nx) + 1;
+#pragma unroll
+    for (int q = 0; q < 5; q++) Q[q][G.ih(i, j, kdst)] = Q[q][G.ih(i, j, ksrc)];
+  }
+}
+cudaError_t launch_bc_layer(const Grid& g, const Phys& ph, const BcLayer& bl, double* const prim[5], cudaStream_t st) {
+  double *d = prim[0], *u = prim[1], *v = prim[2], *w = prim[3], *T = prim[4];
+  k_bcl_inlet<<<148, 256, 0, st>>>(g, ph, bl, d, u, v, w, T);
+  k_bcl_upper<<<148, 256, 0, st>>>(g, ph, bl, d, u, v, w, T);
+  k_bcl_wall<<<148, 256, 0, st>>>(g, ph, bl, d, u, v, w, T);
+  const int outlet = (int)llrint(ph.ibc == 3 ? ph.bc_p[0] : ph.bc_p[3]);
+  if (outlet == 1 || outlet == 2) k_bcl_outlet<<<148, 256, 0, st>>>(g, outlet, d, u, v, w, T);
+  if (ph.ibc == 3) {
+    if (llrint(ph.bc_p[10]) == 1) k_bcl_zside<<<148, 256, 0, st>>>(g, 1, 2, d, u, v, w, T);
+    if (llrint(ph.bc_p[11]) == 1) k_bcl_zside<<<148, 256, 0, st>>>(g, g.nz, g.nz - 1, d, u, v, w, T);
+  }
+  return cudaGetLastError();
+}
+
+// init_bc_nonRef: mode 0 automatic (Dirichlet where the upper boundary's slope
+// dy/dx >= tan(AoA) + 1e-6), 1 non-reflecting everywhere, 2 Dirichlet everywhere.
+__global__ void k_bcl_mask(Grid G, const double* axx, const double* ayy, int mode, double sy0, int* mask) {
+  const long long tot = (long long)G.nx * G.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % G.nx) + 1, k = (int)(t / G.nx) + 1;
+    int dir = 0;
+    if (mode == 2) {
+      dir = 1;
+    } else if (mode == 0) {
+      const int ia = i == 1 ? i + 1 : i, ib = i == 1 ? i : i - 1;
+      const double sy = (ayy[G.ih(ia, G.ny, k)] - ayy[G.ih(ib, G.ny, k)]) / (axx[G.ih(ia, G.ny, k)] - axx[G.ih(ib, G.ny, k)]);
+      dir = sy >= sy0 + 1.0e-6;
+    }
+    mask[t] = dir;
+  }
+}
+cudaError_t launch_bc_layer_mask(const Grid& g, const double* axx, const double* ayy, int mode, double sy0, int* mask,
+                                 cudaStream_t st) {
+  k_bcl_mask<<<148, 256, 0, st>>>(g, axx, ayy, mode, sy0, mask);
+  return cudaGetLastError();
+}
+
+// Flow_Ghost_Userdef (OCFD_GhostCell_UserDef.f90:13-20): swept corner k- symmetry
+// (Flow_Ghost_Sweptcorner :54-73) and flat-plate j- extrapolation with the
+// limiter [0.5, 2] (Flow_Ghost_flatplate :106-136).
+__global__ void k_ghost_user(Grid G, Phys ph, double* d, double* u, double* v, double* w, double* T) {
+  const bool sc = ph.ibc == 3 && ph.ghost[4] == -1;
+  const long long tot = sc ? (long long)G.nx * G.ny * LAP : (long long)G.nx * G.nz * LAP;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    if (sc) {
+      const int i = (int)(t % G.nx) + 1, j = (int)((t / G.nx) % G.ny) + 1, k = 1 - LAP + (int)(t / ((long long)G.nx * G.ny));
+      const long long h = G.ih(i, j, k), h1 = G.ih(i, j, 1 - k);
+      u[h] = u[h1];
+      v[h] = v[h1];
+      w[h] = -w[h1];
+      d[h] = d[h1];
+      T[h] = T[h1];
+    } else {
+      const double s1 = 0.5, s2 = 2.0;
+      const int i = (int)(t % G.nx) + 1, k = (int)((t / G.nx) % G.nz) + 1, j = 1 - LAP + (int)(t / ((long long)G.nx * G.nz));
+      const long long h = G.ih(i, j, k), hw = G.ih(i, 1, k), h1 = G.ih(i, 2 - j, k);
+      u[h] = 2.0 * u[hw] - u[h1];
+      v[h] = 2.0 * v[hw] - v[h1];
+      w[h] = 2.0 * w[hw] - w[h1];
+      double dg = 2.0 * d[hw] - d[h1];
+      double Tg = 2.0 * T[hw] - T[h1];
+      if (dg < s1 * d[hw]) dg = s1 * d[hw];
+      if (dg > s2 * d[hw]) dg = s2 * d[hw];
+      if (Tg < s1 * T[hw]) Tg = s1 * T[hw];
+      if (Tg > s2 * T[hw]) Tg = s2 * T[hw];
+      d[h] = dg;
+      T[h] = Tg;
+    }
+  }
+}
+
 // Flow_Ghost_Extent_2nd (OCFD_GhostCell.f90:164-286): mirror extrapolation with
 // the density/temperature limiter [0.8, 1.2] of the boundary value.
 __global__ void k_ghost(Grid G, Phys ph, double* d, double* u, double* v, double* w, double* T) {
@@ -779,8 +955,9 @@ __global__ void k_ghost(Grid G, Phys ph, double* d, double* u, double* v, double
 cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st) {
   bool any = false;
   for (int f = 0; f < 6; f++) any = any || ph.ghost[f] == 1 || ph.ghost[f] == 2;
-  if (!any) return cudaSuccess;
-  k_ghost<<<148 * 2, 256, 0, st>>>(g, ph, prim[0], prim[1], prim[2], prim[3], prim[4]);
+  if (any) k_ghost<<<148 * 2, 256, 0, st>>>(g, ph, prim[0], prim[1], prim[2], prim[3], prim[4]);
+  if ((ph.ibc == 3 && ph.ghost[4] == -1) || (ph.ibc == 2 && ph.ghost[2] == -1))
+    k_ghost_user<<<148 * 2, 256, 0, st>>>(g, ph, prim[0], prim[1], prim[2], prim[3], prim[4]);
   return cudaGetLastError();
 }
 

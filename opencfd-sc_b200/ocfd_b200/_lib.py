@@ -36,6 +36,13 @@ class NegativeTemperatureStop(OcfdError):
     """The reference stops when more than 10 points have T <= 0 in one stage."""
 
 
+class OcfdBcLayer(C.Structure):
+    """ocfd_bc_layer of include/ocfd_gpu.h."""
+    _fields_ = [("inlet", C.POINTER(C.c_double)), ("upper", C.POINTER(C.c_double)),
+                ("pertb", C.POINTER(C.c_double)), ("mt", C.c_int32), ("beta", C.c_double),
+                ("tm", C.POINTER(C.c_double)), ("fait", C.POINTER(C.c_double))]
+
+
 def _declare(L: C.CDLL) -> C.CDLL:
     P = C.POINTER(OcfdParams)
     H = C.c_void_p
@@ -95,6 +102,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_batch_step.restype = C.c_int
     L.ocfd_batch_destroy.argtypes = [H]
     L.ocfd_batch_destroy.restype = None
+    L.ocfd_gpu_set_bc_layer.argtypes = [H, C.POINTER(OcfdBcLayer)]
+    L.ocfd_gpu_set_bc_layer.restype = C.c_int
     L.ocfd_gpu_metric_zero_mask.argtypes = [H]
     L.ocfd_gpu_metric_zero_mask.restype = C.c_uint
     L.ocfd_batch_set_tiles.argtypes = [H, C.POINTER(C.c_int)]
@@ -130,4 +139,5 @@ EXPORTED = [
     "ocfd_gpu_advance_clock", "ocfd_gpu_step", "ocfd_gpu_show_flow_msg", "ocfd_gpu_ana_box", "ocfd_batch_create",
     "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps", "ocfd_show_flow_msg_noalloc",
     "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error", "ocfd_gpu_metric_zero_mask",
+    "ocfd_gpu_set_bc_layer",
 ]

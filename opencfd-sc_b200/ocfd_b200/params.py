@@ -17,7 +17,7 @@ SCHEME = {"WENO5": 1, "WENO7": 2, "OMP6": 3, "UD7L": 4, "CD6": 5, "CD8": 6, "HYB
 SCHEME_WENO5, SCHEME_WENO7, SCHEME_OMP6, SCHEME_UD7L, SCHEME_CD6, SCHEME_CD8, SCHEME_HYBRID = 1, 2, 3, 4, 5, 6, 10
 SPLIT_SW, SPLIT_LLF = 1, 2
 BC = {"BC_NONE": 0, "BC_BLUNT2D": 1, "BC_BOUNDARYLAYER": 2, "BC_SWEPTCORNER": 3, "BC_USER_DEF": 99}
-BC_NONE, BC_BLUNT2D, BC_USER_DEF = 0, 1, 99
+BC_NONE, BC_BLUNT2D, BC_BOUNDARYLAYER, BC_SWEPTCORNER, BC_USER_DEF = 0, 1, 2, 3, 99
 GRIDGEN, GRID1D, GRID2D_PLANE, GRID2D_AXIAL_SYMM, GRID3D, GRID_AND_JACOBIAN3D = 0, 10, 20, 21, 30, 31
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 

@@ -96,6 +96,15 @@ class Solver:
         arr = (C.POINTER(C.c_double) * 22)(*[_dp(m) for m in ms])
         self._check(self.L.ocfd_gpu_upload_metrics(self.h, arr), "upload_metrics")
 
+    def set_bc_layer(self, data):
+        """Boundary data of BC_BoundaryLayer / BC_SweptCorner (ocfd_b200.bclayer.BcLayerData)."""
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (data.inlet, data.upper, data.pertb, data.tm, data.fait)]
+        ptr = lambda a: None if a is None or a.size == 0 else _dp(a)
+        d = _lib.OcfdBcLayer(ptr(keep[0]), ptr(keep[1]), ptr(keep[2]), len(data.tm), data.beta, ptr(keep[3]),
+                             ptr(keep[4]))
+        self._check(self.L.ocfd_gpu_set_bc_layer(self.h, C.byref(d)), "set_bc_layer")
+
     def metric_zero_mask(self) -> int:
         """Bit m: metric m is identically +0.0 where the kernels read it (loads skipped)."""
         return int(self.L.ocfd_gpu_metric_zero_mask(self.h))

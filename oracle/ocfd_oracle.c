@@ -46,6 +46,11 @@ struct ocfd_oracle {
   struct pwork* pw;
   int istep;
   double tt;
+  /* BC_BoundaryLayer / BC_SweptCorner data (BC_data, OCFD_BC_Boundarylayers.f90:3-15) */
+  double *bl_inlet, *bl_upper, *bl_pertb, *bl_tm, *bl_fait;
+  int *bl_dirichlet;
+  int bl_mt;
+  double bl_beta;
 };
 
 /* ---------------------------------------------------------------- indexing */
@@ -581,6 +586,8 @@ void orc_destroy(ocfd_oracle* o) {
     free(w->ph1); free(w->ph2); free(w->scm);
   }
   free(o->pw);
+  free(o->bl_inlet); free(o->bl_upper); free(o->bl_pertb); free(o->bl_tm); free(o->bl_fait);
+  free(o->bl_dirichlet);
   free(o);
 }
 
@@ -878,6 +885,8 @@ static void jac_ghost_extent_2nd(ocfd_oracle* o) {
 
 /* init_mesh: OCFD_mesh.f90:1-58.  x,y,z NULL -> mesh_gen('box') (:319-354);
  * otherwise interior coordinates as read by read_mesh1d/2d_plane/3d. */
+static void jac_ghost_user(ocfd_oracle* o);
+
 void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const double* z) {
   double** M = o->met;
   const double PI = 3.1415926535897932;
@@ -901,13 +910,48 @@ void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const doubl
   updata_axyz_periodic(o);
   comput_jacobian3d(o);
   for (int m = OCFD_M_AKX; m <= OCFD_M_AJAC; m++) orc_exchange_xyz(o, M[m]);
-  /* Jac_Ghost_boundary: OCFD_GhostCell.f90:1-7 (the user-defined part only
-   * serves BC_SweptCorner / BC_BoundaryLayer, which are not in scope) */
+  /* Jac_Ghost_boundary: OCFD_GhostCell.f90:1-7 */
   jac_ghost_extent_1st(o);
   jac_ghost_extent_2nd(o);
+  jac_ghost_user(o);
   for (size_t h = 0; h < o->nh; h++) {
     double J = M[OCFD_M_AJAC][h];
     for (int m = 0; m < 9; m++) M[OCFD_M_AKX1 + m][h] = M[OCFD_M_AKX + m][h] / J;
+  }
+}
+
+/* Jac_Ghost_Userdef: OCFD_GhostCell_UserDef.f90:4-11 with Jac_Ghost_Sweptcorner
+ * (:23-49, k- symmetry about z = 0) and Jac_Ghost_flatplate (:76-102, j-
+ * symmetry about y = 0): mirrored metrics, sign flips of the reflected components */
+static void jac_ghost_user(ocfd_oracle* o) {
+  double** M = o->met;
+  if (o->p.ibc == OCFD_BC_SWEPTCORNER && o->p.ghost_cell[4] == -1) {
+    /* sign of Akx..Ajac, Axx..Azz under z -> -z */
+    const int ids[13] = {OCFD_M_AKX, OCFD_M_AKY, OCFD_M_AKZ, OCFD_M_AIX, OCFD_M_AIY, OCFD_M_AIZ, OCFD_M_ASX,
+                         OCFD_M_ASY, OCFD_M_ASZ, OCFD_M_AJAC, OCFD_M_AXX, OCFD_M_AYY, OCFD_M_AZZ};
+    const double sg[13] = {1, 1, -1, 1, 1, -1, -1, -1, 1, 1, 1, 1, -1};
+    for (int k = 1 - LAP; k <= 0; k++) {
+      int k1 = 1 - k;
+      for (int j = 1; j <= o->ny; j++)
+        for (int i = 1; i <= o->nx; i++)
+          for (int q = 0; q < 13; q++) {
+            double x = M[ids[q]][IH(o, i, j, k1)];
+            M[ids[q]][IH(o, i, j, k)] = sg[q] < 0 ? -x : x;
+          }
+    }
+  } else if (o->p.ibc == OCFD_BC_BOUNDARYLAYER && o->p.ghost_cell[2] == -1) {
+    const int ids[13] = {OCFD_M_AKX, OCFD_M_AKY, OCFD_M_AKZ, OCFD_M_AIX, OCFD_M_AIY, OCFD_M_AIZ, OCFD_M_ASX,
+                         OCFD_M_ASY, OCFD_M_ASZ, OCFD_M_AJAC, OCFD_M_AXX, OCFD_M_AYY, OCFD_M_AZZ};
+    const double sg[13] = {1, -1, 1, -1, 1, -1, 1, -1, 1, 1, 1, -1, 1};
+    for (int k = 1; k <= o->nz; k++)
+      for (int j = 1 - LAP; j <= 0; j++) {
+        int j1 = 2 - j;
+        for (int i = 1; i <= o->nx; i++)
+          for (int q = 0; q < 13; q++) {
+            double x = M[ids[q]][IH(o, i, j1, k)];
+            M[ids[q]][IH(o, i, j, k)] = sg[q] < 0 ? -x : x;
+          }
+      }
   }
 }
 
@@ -945,6 +989,206 @@ static void bc_user_isothermal(ocfd_oracle* o) {
       size_t h = IH(o, i, o->ny, k);
       o->d[h] = 1.0; o->u[h] = 1.0; o->v[h] = 0.0; o->w[h] = 0.0; o->T[h] = 1.0;
     }
+}
+
+/* ---- BC_BoundaryLayer / BC_SweptCorner (OCFD_BC_Boundarylayers.f90) ----
+ * The boundary data that the reference builds at its first call
+ * (init_bcdata_boundarylayer :171-270 reads the inlet / upper files,
+ * init_bc_wall_perturbation :313-400 draws random phases) arrive from the host:
+ * inlet (ny,nz,5), upper (nx,nz,5), wall perturbation shape (nx,nz), and the
+ * amplitudes TM / phases fait of the time factor (get_ht_multifrequancy
+ * :404-440).  init_bc_nonRef (:273-311) is computed here from the grid. */
+void orc_set_bc_layer(ocfd_oracle* o, const double* inlet, const double* upper, const double* pertb, int mt,
+                      double beta, const double* tm, const double* fait) {
+  const size_t ni = (size_t)o->ny * o->nz * 5, nu = (size_t)o->nx * o->nz * 5, np = (size_t)o->nx * o->nz;
+  free(o->bl_inlet); free(o->bl_upper); free(o->bl_pertb); free(o->bl_tm); free(o->bl_fait);
+  free(o->bl_dirichlet);
+  o->bl_inlet = (double*)calloc(ni, sizeof(double));
+  o->bl_upper = (double*)calloc(nu, sizeof(double));
+  o->bl_pertb = (double*)calloc(np, sizeof(double));
+  o->bl_dirichlet = (int*)calloc(np, sizeof(int));
+  o->bl_mt = mt > 0 ? mt : 0;
+  o->bl_beta = beta;
+  o->bl_tm = (double*)calloc((size_t)o->bl_mt + 1, sizeof(double));
+  o->bl_fait = (double*)calloc((size_t)o->bl_mt + 1, sizeof(double));
+  if (inlet) memcpy(o->bl_inlet, inlet, ni * sizeof(double));
+  if (upper) memcpy(o->bl_upper, upper, nu * sizeof(double));
+  if (pertb) memcpy(o->bl_pertb, pertb, np * sizeof(double));
+  for (int m = 0; m < o->bl_mt; m++) { o->bl_tm[m] = tm[m]; o->bl_fait[m] = fait[m]; }
+  /* init_bc_nonRef: mode 0 auto (Dirichlet where the upper boundary rises faster
+   * than the free stream, tan(AoA)), 1 non-reflecting, 2 Dirichlet */
+  const int mode = o->p.ibc == OCFD_BC_SWEPTCORNER ? 0 : (int)lround(o->p.bc_para[2]);
+  const double sy0 = tan(o->p.aoa), epsl = 1.0e-6;
+  double** M = o->met;
+  for (int k = 1; k <= o->nz; k++)
+    for (int i = 1; i <= o->nx; i++) {
+      int dir = 0;
+      if (mode == 2) dir = 1;
+      else if (mode == 0) {
+        double sy;
+        if (i == 1)
+          sy = (M[OCFD_M_AYY][IH(o, i + 1, o->ny, k)] - M[OCFD_M_AYY][IH(o, i, o->ny, k)]) /
+               (M[OCFD_M_AXX][IH(o, i + 1, o->ny, k)] - M[OCFD_M_AXX][IH(o, i, o->ny, k)]);
+        else
+          sy = (M[OCFD_M_AYY][IH(o, i, o->ny, k)] - M[OCFD_M_AYY][IH(o, i - 1, o->ny, k)]) /
+               (M[OCFD_M_AXX][IH(o, i, o->ny, k)] - M[OCFD_M_AXX][IH(o, i - 1, o->ny, k)]);
+        dir = sy >= sy0 + epsl;
+      }
+      o->bl_dirichlet[(size_t)(i - 1) + (size_t)o->nx * (k - 1)] = dir;
+    }
+}
+
+/* get_ht_multifrequancy: OCFD_BC_Boundarylayers.f90:404-440 */
+static double bl_ht(const ocfd_oracle* o) {
+  const double PI = 3.14159265358979;
+  if (!(o->bl_beta > 0.0)) return 1.0;
+  double ht = 0.0;
+  for (int m = 1; m <= o->bl_mt; m++) ht = ht + o->bl_tm[m - 1] * sin(m * o->bl_beta * o->tt + 2.0 * PI * o->bl_fait[m - 1]);
+  return ht;
+}
+
+static void bl_set(ocfd_oracle* o, size_t h, double d, double u, double v, double w, double T) {
+  o->d[h] = d; o->u[h] = u; o->v[h] = v; o->w[h] = w; o->T[h] = T;
+}
+
+/* the j=1 wall of both BCs (:123-141, :525-551) for point (i,k) */
+static void bl_wall(ocfd_oracle* o, int i, int k, double Tw, double A, double ht) {
+  double** M = o->met;
+  size_t h1 = IH(o, i, 1, k), h2 = IH(o, i, 2, k), h3 = IH(o, i, 3, k);
+  double aix = M[OCFD_M_AIX][h1], aiy = M[OCFD_M_AIY][h1], aiz = M[OCFD_M_AIZ][h1];
+  double tmp = 1.0 / (sqrt(aix * aix + aiy * aiy + aiz * aiz));
+  double A0 = A * ht * o->bl_pertb[(size_t)(i - 1) + (size_t)o->nx * (k - 1)];
+  o->u[h1] = A0 * aix * tmp;
+  o->v[h1] = A0 * aiy * tmp;
+  o->w[h1] = A0 * aiz * tmp;
+  if (Tw > 0.0) {
+    o->T[h1] = Tw;
+    o->d[h1] = (4.0 * o->d[h2] * o->T[h2] - o->d[h3] * o->T[h3]) / (3.0 * Tw);
+  } else {
+    o->T[h1] = (4.0 * o->T[h2] - o->T[h3]) / 3.0;
+    o->d[h1] = (4.0 * o->d[h2] - o->d[h3]) / 3.0;
+  }
+}
+
+/* outlet i=nx (:143-167): 1 first-order, 2 second-order extrapolation */
+static void bl_outlet(ocfd_oracle* o, int mode) {
+  double* Q[5] = {o->d, o->u, o->v, o->w, o->T};
+  if (mode != 1 && mode != 2) return;
+  for (int k = 1; k <= o->nz; k++)
+    for (int j = 1; j <= o->ny; j++) {
+      size_t h = IH(o, o->nx, j, k), h1 = IH(o, o->nx - 1, j, k), h2 = IH(o, o->nx - 2, j, k);
+      for (int q = 0; q < 5; q++) Q[q][h] = mode == 1 ? Q[q][h1] : 2.0 * Q[q][h1] - Q[q][h2];
+    }
+}
+
+static void bl_upper(ocfd_oracle* o, int data) {
+  const double u0 = cos(o->p.aoa), v0 = sin(o->p.aoa);
+  for (int k = 1; k <= o->nz; k++)
+    for (int i = 1; i <= o->nx; i++) {
+      const size_t c = (size_t)(i - 1) + (size_t)o->nx * (k - 1), nxz = (size_t)o->nx * o->nz;
+      if (!o->bl_dirichlet[c]) continue;
+      size_t h = IH(o, i, o->ny, k);
+      if (data == 0)
+        bl_set(o, h, 1.0, u0, v0, 0.0, 1.0);
+      else {
+        const double* U = o->bl_upper;
+        bl_set(o, h, U[c], U[c + nxz], U[c + 2 * nxz], U[c + 3 * nxz], U[c + 4 * nxz]);
+      }
+    }
+}
+
+/* ocfd_bc_BoundaryLayer: OCFD_BC_Boundarylayers.f90:17-169 */
+static void bc_boundary_layer(ocfd_oracle* o) {
+  const double* bp = o->p.bc_para;
+  const int inlet = (int)lround(bp[0]), upper = (int)lround(bp[1]), outlet = (int)lround(bp[3]);
+  const double Tw = bp[4], A = bp[7];
+  const double u0 = cos(o->p.aoa), v0 = sin(o->p.aoa);
+  /* inlet i=1: the free stream of the reference sets T = 0 there (:58-66) */
+  for (int k = 1; k <= o->nz; k++)
+    for (int j = 1; j <= o->ny; j++) {
+      size_t h = IH(o, 1, j, k);
+      if (inlet == 0)
+        bl_set(o, h, 1.0, u0, v0, 0.0, 0.0);
+      else {
+        const size_t c = (size_t)(j - 1) + (size_t)o->ny * (k - 1), nyz = (size_t)o->ny * o->nz;
+        const double* I = o->bl_inlet;
+        bl_set(o, h, I[c], I[c + nyz], I[c + 2 * nyz], I[c + 3 * nyz], I[c + 4 * nyz]);
+      }
+    }
+  bl_upper(o, upper);
+  const double ht = bl_ht(o);
+  for (int k = 1; k <= o->nz; k++)
+    for (int i = 1; i <= o->nx; i++) bl_wall(o, i, k, Tw, A, ht);
+  bl_outlet(o, outlet);
+}
+
+/* ocfd_bc_swept_corner: OCFD_BC_Boundarylayers.f90:443-618 (1-D inlet data,
+ * free-stream upper boundary with the automatic Dirichlet mask) */
+static void bc_swept_corner(ocfd_oracle* o) {
+  const double* bp = o->p.bc_para;
+  const int outlet = (int)lround(bp[0]), z1 = (int)lround(bp[10]), z2 = (int)lround(bp[11]);
+  const double Tw = bp[1], wall_zl = bp[2], A = bp[4], epsl = 1.0e-7;
+  double** M = o->met;
+  double* Q[5] = {o->d, o->u, o->v, o->w, o->T};
+  for (int k = 1; k <= o->nz; k++)
+    for (int j = 1; j <= o->ny; j++) {
+      const size_t c = (size_t)(j - 1) + (size_t)o->ny * (k - 1), nyz = (size_t)o->ny * o->nz;
+      const double* I = o->bl_inlet;
+      bl_set(o, IH(o, 1, j, k), I[c], I[c + nyz], I[c + 2 * nyz], I[c + 3 * nyz], I[c + 4 * nyz]);
+    }
+  bl_upper(o, 0);
+  const double ht = bl_ht(o);
+  for (int k = 1; k <= o->nz; k++)
+    for (int i = 1; i <= o->nx; i++) {
+      size_t h1 = IH(o, i, 1, k), h2 = IH(o, i, 2, k);
+      double zz = M[OCFD_M_AZZ][h1], yy = M[OCFD_M_AYY][h1];
+      if ((zz >= -epsl && zz <= wall_zl + epsl) || yy <= epsl)
+        bl_wall(o, i, k, Tw, A, ht);
+      else
+        for (int q = 0; q < 5; q++) Q[q][h1] = Q[q][h2];
+    }
+  bl_outlet(o, outlet);
+  if (z1 == 1)
+    for (int j = 1; j <= o->ny; j++)
+      for (int i = 1; i <= o->nx; i++)
+        for (int q = 0; q < 5; q++) Q[q][IH(o, i, j, 1)] = Q[q][IH(o, i, j, 2)];
+  if (z2 == 1)
+    for (int j = 1; j <= o->ny; j++)
+      for (int i = 1; i <= o->nx; i++)
+        for (int q = 0; q < 5; q++) Q[q][IH(o, i, j, o->nz)] = Q[q][IH(o, i, j, o->nz - 1)];
+}
+
+/* Flow_Ghost_Userdef: OCFD_GhostCell_UserDef.f90:13-20, 54-73 (swept corner,
+ * k- symmetry) and 106-136 (flat plate, j- extrapolation with limiter) */
+static void flow_ghost_user(ocfd_oracle* o) {
+  if (o->p.ibc == OCFD_BC_SWEPTCORNER && o->p.ghost_cell[4] == -1) {
+    for (int k = 1 - LAP; k <= 0; k++) {
+      int k1 = 1 - k;
+      for (int j = 1; j <= o->ny; j++)
+        for (int i = 1; i <= o->nx; i++) {
+          size_t h = IH(o, i, j, k), h1 = IH(o, i, j, k1);
+          o->u[h] = o->u[h1]; o->v[h] = o->v[h1]; o->w[h] = -o->w[h1]; o->d[h] = o->d[h1]; o->T[h] = o->T[h1];
+        }
+    }
+  } else if (o->p.ibc == OCFD_BC_BOUNDARYLAYER && o->p.ghost_cell[2] == -1) {
+    const double s1 = 0.5, s2 = 2.0;
+    for (int k = 1; k <= o->nz; k++)
+      for (int j = 1 - LAP; j <= 0; j++) {
+        int j1 = 2 - j;
+        for (int i = 1; i <= o->nx; i++) {
+          size_t h = IH(o, i, j, k), hw = IH(o, i, 1, k), h1 = IH(o, i, j1, k);
+          o->u[h] = 2.0 * o->u[hw] - o->u[h1];
+          o->v[h] = 2.0 * o->v[hw] - o->v[h1];
+          o->w[h] = 2.0 * o->w[hw] - o->w[h1];
+          o->d[h] = 2.0 * o->d[hw] - o->d[h1];
+          o->T[h] = 2.0 * o->T[hw] - o->T[h1];
+          if (o->d[h] < s1 * o->d[hw]) o->d[h] = s1 * o->d[hw];
+          if (o->d[h] > s2 * o->d[hw]) o->d[h] = s2 * o->d[hw];
+          if (o->T[h] < s1 * o->T[hw]) o->T[h] = s1 * o->T[hw];
+          if (o->T[h] > s2 * o->T[hw]) o->T[h] = s2 * o->T[hw];
+        }
+      }
+  }
 }
 
 /* Flow_Ghost_Extent_2nd: OCFD_GhostCell.f90:164-286 */
@@ -986,6 +1230,8 @@ static void flow_ghost_extent_2nd(ocfd_oracle* o) {
 void orc_bc(ocfd_oracle* o) {
   if (o->p.ibc == OCFD_BC_BLUNT2D) bc_blunt2d(o);
   else if (o->p.ibc == OCFD_BC_USER_DEF) bc_user_isothermal(o);
+  else if (o->p.ibc == OCFD_BC_BOUNDARYLAYER) bc_boundary_layer(o);
+  else if (o->p.ibc == OCFD_BC_SWEPTCORNER) bc_swept_corner(o);
   const double Cv = o->p.cv;
   /* f refresh on the six faces, in the reference's order */
   for (int face = 0; face < 6; face++) {
@@ -1007,6 +1253,7 @@ void orc_bc(ocfd_oracle* o) {
       }
   }
   flow_ghost_extent_2nd(o);
+  flow_ghost_user(o);
 }
 
 /* init3d: OCFD_init.f90:1-20, then the OCFD_bc of OCFD_NS_Solver.f90:15 */

@@ -60,6 +60,11 @@ void orc_rk3(ocfd_oracle* o, int krk);
 /* returns number of repaired points, or -1 when the reference would stop */
 int orc_duvwt(ocfd_oracle* o);
 void orc_bc(ocfd_oracle* o);
+/* BC_BoundaryLayer / BC_SweptCorner boundary data (after orc_init_mesh):
+ * inlet (ny,nz,5), upper (nx,nz,5), wall perturbation (nx,nz) -- each may be
+ * NULL for zeros -- and the time factor's amplitudes / phases (mt each). */
+void orc_set_bc_layer(ocfd_oracle* o, const double* inlet, const double* upper, const double* pertb, int mt,
+                      double beta, const double* tm, const double* fait);
 void orc_filtering(ocfd_oracle* o);
 /* one full time step; returns 0 or -1 (negative-T stop) */
 int orc_step(ocfd_oracle* o);

@@ -64,6 +64,7 @@ def lib() -> C.CDLL:
         L.orc_flux1d.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_int, C.POINTER(C.c_int), dp]
         L.orc_char_matrices.argtypes = [C.c_double, dp, dp, dp, dp]
         L.orc_d0.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        L.orc_set_bc_layer.argtypes = [C.c_void_p, dp, dp, dp, C.c_int, C.c_double, dp, dp]
         _lib = L
     return _lib
 
@@ -173,6 +174,16 @@ class Oracle:
 
     def bc(self):
         lib().orc_bc(self.h)
+
+    def set_bc_layer(self, data):
+        """BC_BoundaryLayer / BC_SweptCorner boundary data (ocfd_b200.bclayer.BcLayerData)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (data.inlet, data.upper, data.pertb)]
+        tm = np.ascontiguousarray(data.tm, dtype=np.float64)
+        fait = np.ascontiguousarray(data.fait, dtype=np.float64)
+        self._bl = (arrs, tm, fait)
+        lib().orc_set_bc_layer(self.h, *[None if a is None else _dp(a) for a in arrs], len(tm), data.beta,
+                               _dp(tm) if len(tm) else None, _dp(fait) if len(fait) else None)
 
     def filtering(self):
         lib().orc_filtering(self.h)

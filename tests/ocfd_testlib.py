@@ -58,3 +58,59 @@ def rel_l2(a, b):
 
 def interior(h):
     return h[LAP:-LAP, LAP:-LAP, LAP:-LAP]
+
+
+def boundary_layer_case(kind="bl", n=(24, 20, 8), ghost=False, tw=-1.0, pert=True, nonref=0, outlet=2,
+                        inlet_2d=False, ma=2.25, re=1.0e4, dt=5.0e-4, seed=11):
+    """Flat-plate boundary layer (BC_BoundaryLayer, kind "bl", periodic span) or
+    swept-corner style span (BC_SweptCorner, kind "sc": walls on part of the
+    span, k- symmetry plane).  2-D plane grid: x uniform in [0.1, 1.1], y
+    sinh-stretched in [0, 0.4]; span uniform.  Inlet and initial field: a
+    synthetic compressible boundary-layer profile (u = tanh(3 y / 0.1), adiabatic
+    Crocco temperature, constant pressure)."""
+    from ocfd_b200 import bclayer
+    from ocfd_b200.params import BC_BOUNDARYLAYER, BC_SWEPTCORNER, GRID2D_PLANE, SCHEME_WENO7, default_params
+
+    ni, nj, nk = n
+    p = default_params()
+    p.nx, p.ny, p.nz = ni, nj, nk
+    p.iperiodic[0] = p.iperiodic[1] = 0
+    p.iperiodic[2] = 1 if kind == "bl" else 0
+    lz = 0.2
+    p.periodic_span[2][2] = lz
+    p.iflag_gridtype = GRID2D_PLANE
+    p.scheme_invis = SCHEME_WENO7
+    p.if_scheme_character = 1
+    p.ma, p.re, p.dt = ma, re, dt
+    p.ibc = BC_BOUNDARYLAYER if kind == "bl" else BC_SWEPTCORNER
+    x = 0.1 + np.arange(ni) / (ni - 1.0)
+    b = 2.5
+    y = 0.4 * np.sinh(b * np.arange(nj) / (nj - 1.0)) / np.sinh(b)
+    dz = lz / nk
+    z = (np.arange(nk) + 0.5) * dz if kind == "sc" else np.arange(nk) * dz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    u = np.tanh(3.0 * y / 0.1)
+    T = 1.0 + 0.89 * 0.2 * ma * ma * (1.0 - u * u)
+    prof = np.stack([1.0 / T, u, np.zeros_like(u), np.zeros_like(u), T], axis=1)  # (ny, 5)
+    prims = [np.ascontiguousarray(np.broadcast_to(prof[:, q][None, :, None], (nk, nj, ni))) for q in range(5)]
+    rng = np.random.default_rng(seed)
+    inlet = bclayer.inlet_from_profile(prof, nk)
+    if inlet_2d:
+        inlet = inlet * (1.0 + 0.01 * np.cos(2 * np.pi * np.arange(nk) / nk))[None, :, None]
+    if kind == "bl":
+        bclayer.boundary_layer_bc_para(p, inlet=2 if inlet_2d else 1, upper=0, nonref=nonref, outlet=outlet, tw=tw,
+                                       dis_type=1 if pert else 0, amp=0.02, xbegin=0.3, xend=0.8, mt=3, mz=2,
+                                       zl=lz, freq=20.0)
+        if ghost:
+            p.ghost_cell[2] = -1
+            p.scheme_boundary[2] = -1
+        pertb = bclayer.wall_perturbation(1 if pert else 0, X[:, 0, :], Z[:, 0, :], 0.3, 0.8, 2, lz, rng)
+    else:
+        bclayer.swept_corner_bc_para(p, outlet=outlet, tw=tw, wall_zl=0.5 * lz, dis_type=1 if pert else 0,
+                                     amp=0.02, xbegin=0.3, xend=0.8, mt=3, mz=-1, freq=20.0, z1=0, z2=1)
+        p.ghost_cell[4] = -1
+        p.scheme_boundary[4] = -1
+        pertb = bclayer.wall_perturbation(1 if pert else 0, X[:, 0, :], Z[:, 0, :], 0.3, 0.8, -1, 0.5 * lz, rng)
+    tm, fait = bclayer.time_factor(3, rng)
+    data = bclayer.BcLayerData(inlet=inlet, pertb=pertb, beta=20.0 if pert else 0.0, tm=tm, fait=fait)
+    return p, (X, Y, Z), prims, data

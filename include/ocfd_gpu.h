@@ -303,6 +303,25 @@ int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]);
  * d_rms, T_aver, Amu_aver, d_aver, Ux_rms, Alamdax. */
 int ocfd_gpu_ana_box(ocfd_handle* h, double out[20]);
 
+/* The other analyses of OCFD_analysis (OCFD_ANA.f90:3-31); the host keeps the
+ * schedule (ANA_Para) and the files.
+ * ana_getQ (OCFD_ANA.f90:127-171): q receives Q = II(grad u), nx*ny*nz. */
+int ocfd_gpu_ana_q(ocfd_handle* h, double* q);
+/* ana_time_average (OCFD_ANA.f90:34-125): adds the current d,u,v,w,T to the
+ * running means (K_average += 1, t_average += dt).  The means start at zero,
+ * or from ocfd_gpu_upload_average (the reference's opencfd.dat.average). */
+int ocfd_gpu_ana_time_average(ocfd_handle* h);
+int ocfd_gpu_download_average(ocfd_handle* h, double* const mean[5], int* k_average, double* t_average);
+int ocfd_gpu_upload_average(ocfd_handle* h, const double* const mean[5], int k_average, double t_average);
+/* Ana_corner (OCFD_ANA.f90:316-384): out[3*nx] = span averages of the
+ * wall-tangential velocity at j=2, of T at j=2 and of the wall pressure. */
+int ocfd_gpu_ana_corner(ocfd_handle* h, double* out);
+/* The interior box [ib,ie]x[jb,je]x[kb,ke] (1-based, inclusive) of d,u,v,w,T,
+ * i fastest (entries of out may be NULL): the data of ana_savedata's planes,
+ * points and blocks (OCFD_ANA_savedata.f90:3-196, write_2d_*a / write_points /
+ * write_blockdata, OCFD_IO_mpi.f90:7-130,286-326). */
+int ocfd_gpu_download_block(ocfd_handle* h, int ib, int ie, int jb, int je, int kb, int ke, double* const out[5]);
+
 /* show_flow_msg on arrays the caller owns, allocating nothing.  No counterpart
  * in the reference: it is for callers that cannot allocate device memory (a
  * host solver whose device memory all belongs to its own pool, or code that

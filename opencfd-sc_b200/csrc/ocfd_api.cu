@@ -67,6 +67,10 @@ struct ocfd_handle {
   bool bl_time_dep = false;  // the wall condition changes with tt: no captured step graphs
   double bl_beta = 0.0;
   std::vector<double> bl_tm, bl_fait;
+  // ana_time_average state: running means of d,u,v,w,T (5 n), samples, time span
+  double* avg = nullptr;
+  int avg_k = 0;
+  double avg_t = 0.0;
   int istep = 0;
   double tt = 0.0;
   std::string err;
@@ -328,6 +332,7 @@ void ocfd_gpu_destroy(ocfd_handle* h) {
   F(h->bl_upper);
   F(h->bl_pertb);
   F(h->bl_mask);
+  F(h->avg);
   if (h->hstat) cudaFreeHost(h->hstat);
   if (h->hout) cudaFreeHost(h->hout);
   if (h->st) cudaStreamDestroy(h->st);
@@ -1092,6 +1097,84 @@ int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]) {
   CK(cudaStreamSynchronize(h->st));
   const double N = (double)(h->p.nx * h->p.ny * h->p.nz);
   for (int q = 0; q < 3; q++) E0[q] = h->hout[q] / N;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_ana_q(ocfd_handle* h, double* q) {
+  if (!h || !q) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  int r = halo_all(h);  // exchange_boundary_xyz(u, v, w) of OCFD_ANA.f90:137-139
+  if (r) return r;
+  CK(launch_ana_q(h->g, h->ph, h->dc, h->prim, h->met, h->scratch, h->st));
+  CK(cudaMemcpyAsync(q, h->scratch, h->g.n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_ana_time_average(ocfd_handle* h) {
+  if (!h) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (!h->avg) {
+    CK(cudaMalloc((void**)&h->avg, 5 * h->g.n * 8));
+    CK(cudaMemsetAsync(h->avg, 0, 5 * h->g.n * 8, h->st));
+    h->avg_k = 0;
+    h->avg_t = 0.0;
+  }
+  CK(launch_ana_average(h->g, h->prim, h->avg, h->avg_k, h->st));
+  h->avg_k += 1;
+  h->avg_t += h->p.dt;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_download_average(ocfd_handle* h, double* const mean[5], int* k_average, double* t_average) {
+  if (!h) return OCFD_E_PARAM;
+  if (!h->avg) return fail(h, OCFD_E_STATE, "no time average taken");
+  CK(cudaSetDevice(h->device));
+  if (mean)
+    for (int q = 0; q < 5; q++)
+      if (mean[q]) CK(cudaMemcpyAsync(mean[q], h->avg + q * h->g.n, h->g.n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (k_average) *k_average = h->avg_k;
+  if (t_average) *t_average = h->avg_t;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_upload_average(ocfd_handle* h, const double* const mean[5], int k_average, double t_average) {
+  if (!h || !mean || k_average < 0) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  if (!h->avg) CK(cudaMalloc((void**)&h->avg, 5 * h->g.n * 8));
+  for (int q = 0; q < 5; q++) {
+    if (!mean[q]) return OCFD_E_PARAM;
+    CK(cudaMemcpyAsync(h->avg + q * h->g.n, mean[q], h->g.n * 8, cudaMemcpyHostToDevice, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  h->avg_k = k_average;
+  h->avg_t = t_average;
+  return OCFD_OK;
+}
+
+int ocfd_gpu_ana_corner(ocfd_handle* h, double* out) {
+  if (!h || !out) return OCFD_E_PARAM;
+  CK(cudaSetDevice(h->device));
+  CK(launch_ana_corner(h->g, h->ph, h->prim, h->met[OCFD_M_AXX], h->met[OCFD_M_AYY], h->scratch, h->st));
+  CK(cudaMemcpyAsync(out, h->scratch, 3 * h->g.nx * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return OCFD_OK;
+}
+
+int ocfd_gpu_download_block(ocfd_handle* h, int ib, int ie, int jb, int je, int kb, int ke, double* const out[5]) {
+  if (!h || !out) return OCFD_E_PARAM;
+  const Grid& g = h->g;
+  if (ib < 1 || jb < 1 || kb < 1 || ie > g.nx || je > g.ny || ke > g.nz || ie < ib || je < jb || ke < kb)
+    return fail(h, OCFD_E_PARAM, "block outside the grid");
+  CK(cudaSetDevice(h->device));
+  const size_t cnt = (size_t)(ie - ib + 1) * (je - jb + 1) * (ke - kb + 1);
+  for (int q = 0; q < 5; q++) {
+    if (!out[q]) continue;
+    CK(launch_gather_box(g, h->prim[q], ib, ie, jb, je, kb, ke, h->scratch, h->st));
+    CK(cudaMemcpyAsync(out[q], h->scratch, cnt * 8, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));  // the scratch is reused by the next variable
+  }
   return OCFD_OK;
 }
 

@@ -669,4 +669,113 @@ cudaError_t launch_ana_box(const Grid& g, const Phys& ph, const DCoef& dc, doubl
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Analysis of OCFD_analysis (OCFD_ANA.f90:3-31) beyond ana_box.
+
+// ana_getQ (OCFD_ANA.f90:127-171): Q = II(grad u) from the CD6/CD8 derivatives of
+// u, v, w (halos exchanged by the caller) and the metrics.
+__global__ void k_ana_q(Grid G, Phys ph, DCoef dc, const double* u, const double* v, const double* w, MetPtrs mp,
+                        double* q) {
+  const int cd8 = ph.scheme_vis == 6;
+  double* const* M = mp.m;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.n; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    decode(G, t, i, j, k);
+    const long long c = G.ih(i, j, k);
+    const long long st[3] = {1, (long long)G.nxh, (long long)G.nxh * G.nyh};
+    const int l[3] = {i, j, k};
+    const double* q3[3] = {u, v, w};
+    double gr[3][3];
+    for (int a = 0; a < 3; a++)
+      for (int dd = 0; dd < 3; dd++) gr[a][dd] = d0h(q3[a] + c, st[dd], l[dd], G.len(dd), ph.periodic[dd], cd8, dc, dd);
+    const double Akx = M[3][c], Aky = M[4][c], Akz = M[5][c], Aix = M[6][c], Aiy = M[7][c], Aiz = M[8][c];
+    const double Asx = M[9][c], Asy = M[10][c], Asz = M[11][c];
+    const double ux = gr[0][0] * Akx + gr[0][1] * Aix + gr[0][2] * Asx;
+    const double vx = gr[1][0] * Akx + gr[1][1] * Aix + gr[1][2] * Asx;
+    const double wx = gr[2][0] * Akx + gr[2][1] * Aix + gr[2][2] * Asx;
+    const double uy = gr[0][0] * Aky + gr[0][1] * Aiy + gr[0][2] * Asy;
+    const double vy = gr[1][0] * Aky + gr[1][1] * Aiy + gr[1][2] * Asy;
+    const double wy = gr[2][0] * Aky + gr[2][1] * Aiy + gr[2][2] * Asy;
+    const double uz = gr[0][0] * Akz + gr[0][1] * Aiz + gr[0][2] * Asz;
+    const double vz = gr[1][0] * Akz + gr[1][1] * Aiz + gr[1][2] * Asz;
+    const double wz = gr[2][0] * Akz + gr[2][1] * Aiz + gr[2][2] * Asz;
+    q[t] = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;
+  }
+}
+cudaError_t launch_ana_q(const Grid& g, const Phys& ph, const DCoef& dc, double* const prim[5],
+                         const double* const met[22], double* q, cudaStream_t st) {
+  MetPtrs mp;
+  for (int m = 0; m < 22; m++) mp.m[m] = const_cast<double*>(met[m]);
+  k_ana_q<<<148 * 8, 256, 0, st>>>(g, ph, dc, prim[1], prim[2], prim[3], mp, q);
+  return cudaGetLastError();
+}
+
+// ana_time_average (OCFD_ANA.f90:34-125): running mean of d, u, v, w, T over the
+// K samples taken so far, mean = (K mean + q) / (K + 1).
+__global__ void k_ana_average(Grid G, const double* d, const double* u, const double* v, const double* w,
+                              const double* T, double* mean, double K) {
+  const double* Q[5] = {d, u, v, w, T};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.n; t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    decode(G, t, i, j, k);
+    const long long c = G.ih(i, j, k);
+    for (int a = 0; a < 5; a++) mean[t + a * G.n] = (K * mean[t + a * G.n] + Q[a][c]) / (K + 1.0);
+  }
+}
+cudaError_t launch_ana_average(const Grid& g, double* const prim[5], double* mean, int K, cudaStream_t st) {
+  k_ana_average<<<148 * 8, 256, 0, st>>>(g, prim[0], prim[1], prim[2], prim[3], prim[4], mean, (double)K);
+  return cudaGetLastError();
+}
+
+// Ana_corner (OCFD_ANA.f90:316-384): per i, span averages of the wall-tangential
+// velocity and temperature at j = 2 and of the wall pressure, in the reference's
+// k order (one thread per i).
+__global__ void k_ana_corner(Grid G, Phys ph, const double* d, const double* u, const double* v, const double* T,
+                             const double* axx, const double* ayy, double* out) {
+  const double p00 = 1.0 / (ph.gamma * ph.ma * ph.ma);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= G.nx; i += gridDim.x * blockDim.x) {
+    double sx, sy;
+    if (i < G.nx) {
+      sx = axx[G.ih(i + 1, 1, 1)] - axx[G.ih(i, 1, 1)];
+      sy = ayy[G.ih(i + 1, 1, 1)] - ayy[G.ih(i, 1, 1)];
+    } else {
+      sx = axx[G.ih(G.nx, 1, 1)] - axx[G.ih(G.nx - 1, 1, 1)];
+      sy = ayy[G.ih(G.nx, 1, 1)] - ayy[G.ih(G.nx - 1, 1, 1)];
+    }
+    const double tmp = 1.0 / sqrt(sx * sx + sy * sy);
+    sx = sx * tmp;
+    sy = sy * tmp;
+    double us = 0.0, Ts = 0.0, ps = 0.0;
+    for (int k = 1; k <= G.nz; k++) {
+      const long long c2 = G.ih(i, 2, k), c1 = G.ih(i, 1, k);
+      us = us + u[c2] * sx + v[c2] * sy;
+      Ts = Ts + T[c2];
+      ps = ps + p00 * d[c1] * T[c1];
+    }
+    const double r = 1.0 / G.nz;
+    out[i - 1] = us * r;
+    out[G.nx + i - 1] = Ts * r;
+    out[2 * G.nx + i - 1] = ps * r;
+  }
+}
+cudaError_t launch_ana_corner(const Grid& g, const Phys& ph, double* const prim[5], const double* axx,
+                              const double* ayy, double* out, cudaStream_t st) {
+  k_ana_corner<<<(g.nx + 255) / 256, 256, 0, st>>>(g, ph, prim[0], prim[1], prim[2], prim[4], axx, ayy, out);
+  return cudaGetLastError();
+}
+
+// A box [ib,ie] x [jb,je] x [kb,ke] (1-based, inclusive) of a haloed array, i fastest.
+__global__ void k_gather_box(Grid G, const double* src, int ib, int jb, int kb, int ni, int nj, int nk, double* dst) {
+  const long long tot = (long long)ni * nj * nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % ni), b = (int)((t / ni) % nj), c = (int)(t / ((long long)ni * nj));
+    dst[t] = src[G.ih(ib + a, jb + b, kb + c)];
+  }
+}
+cudaError_t launch_gather_box(const Grid& g, const double* src, int ib, int ie, int jb, int je, int kb, int ke,
+                              double* dst, cudaStream_t st) {
+  k_gather_box<<<148 * 4, 256, 0, st>>>(g, src, ib, jb, kb, ie - ib + 1, je - jb + 1, ke - kb + 1, dst);
+  return cudaGetLastError();
+}
+
 }  // namespace ocfd

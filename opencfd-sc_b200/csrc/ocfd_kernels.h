@@ -196,6 +196,13 @@ cudaError_t launch_filter(const Grid& g, const Phys& ph, double* f, double* scra
                           cudaStream_t st);
 
 // init_mesh on the device: coords (3 haloed arrays, interior filled) -> metrics
+cudaError_t launch_ana_q(const Grid& g, const Phys& ph, const DCoef& dc, double* const prim[5],
+                         const double* const met[22], double* q, cudaStream_t st);
+cudaError_t launch_ana_average(const Grid& g, double* const prim[5], double* mean, int K, cudaStream_t st);
+cudaError_t launch_ana_corner(const Grid& g, const Phys& ph, double* const prim[5], const double* axx,
+                              const double* ayy, double* out, cudaStream_t st);
+cudaError_t launch_gather_box(const Grid& g, const double* src, int ib, int ie, int jb, int je, int kb, int ke,
+                              double* dst, cudaStream_t st);
 cudaError_t launch_metric_nonzero(const Grid& g, double* const met[22], unsigned int* nonzero, cudaStream_t st);
 cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* const met[22],
                         const double periodic_span[3][3], cudaStream_t st);

@@ -102,6 +102,18 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_batch_step.restype = C.c_int
     L.ocfd_batch_destroy.argtypes = [H]
     L.ocfd_batch_destroy.restype = None
+    L.ocfd_gpu_ana_q.argtypes = [H, dp]
+    L.ocfd_gpu_ana_q.restype = C.c_int
+    L.ocfd_gpu_ana_time_average.argtypes = [H]
+    L.ocfd_gpu_ana_time_average.restype = C.c_int
+    L.ocfd_gpu_download_average.argtypes = [H, C.c_void_p, C.POINTER(C.c_int), dp]
+    L.ocfd_gpu_download_average.restype = C.c_int
+    L.ocfd_gpu_upload_average.argtypes = [H, C.c_void_p, C.c_int, C.c_double]
+    L.ocfd_gpu_upload_average.restype = C.c_int
+    L.ocfd_gpu_ana_corner.argtypes = [H, dp]
+    L.ocfd_gpu_ana_corner.restype = C.c_int
+    L.ocfd_gpu_download_block.argtypes = [H, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    L.ocfd_gpu_download_block.restype = C.c_int
     L.ocfd_gpu_set_bc_layer.argtypes = [H, C.POINTER(OcfdBcLayer)]
     L.ocfd_gpu_set_bc_layer.restype = C.c_int
     L.ocfd_gpu_metric_zero_mask.argtypes = [H]
@@ -139,5 +151,6 @@ EXPORTED = [
     "ocfd_gpu_advance_clock", "ocfd_gpu_step", "ocfd_gpu_show_flow_msg", "ocfd_gpu_ana_box", "ocfd_batch_create",
     "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps", "ocfd_show_flow_msg_noalloc",
     "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error", "ocfd_gpu_metric_zero_mask",
-    "ocfd_gpu_set_bc_layer",
+    "ocfd_gpu_set_bc_layer", "ocfd_gpu_ana_q", "ocfd_gpu_ana_time_average", "ocfd_gpu_download_average",
+    "ocfd_gpu_upload_average", "ocfd_gpu_ana_corner", "ocfd_gpu_download_block",
 ]

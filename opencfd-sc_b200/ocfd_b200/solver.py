@@ -238,6 +238,48 @@ class Solver:
         self._check(self.L.ocfd_gpu_ana_box(self.h, _dp(e)), "ana_box")
         return e
 
+    def ana_q(self) -> np.ndarray:
+        """ana_getQ: the Q criterion, (nz, ny, nx)."""
+        q = np.empty((self.nz, self.ny, self.nx))
+        self._check(self.L.ocfd_gpu_ana_q(self.h, _dp(q)), "ana_q")
+        return q
+
+    def ana_time_average(self):
+        """ana_time_average: add the current d,u,v,w,T to the running means."""
+        self._check(self.L.ocfd_gpu_ana_time_average(self.h), "ana_time_average")
+
+    def download_average(self):
+        """(means [d,u,v,w,T] each (nz, ny, nx), K_average, t_average)."""
+        means = [np.empty((self.nz, self.ny, self.nx)) for _ in range(5)]
+        pp = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in means])
+        k = C.c_int()
+        t = np.zeros(1)
+        self._check(self.L.ocfd_gpu_download_average(self.h, C.cast(pp, C.c_void_p), C.byref(k), _dp(t)),
+                    "download_average")
+        return means, k.value, float(t[0])
+
+    def upload_average(self, means, k_average: int, t_average: float):
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for a in means]
+        pp = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in keep])
+        self._check(self.L.ocfd_gpu_upload_average(self.h, C.cast(pp, C.c_void_p), k_average, t_average),
+                    "upload_average")
+
+    def ana_corner(self) -> np.ndarray:
+        """Ana_corner: (3, nx) span averages u_t(j=2), T(j=2), p_wall."""
+        out = np.empty(3 * self.nx)
+        self._check(self.L.ocfd_gpu_ana_corner(self.h, _dp(out)), "ana_corner")
+        return out.reshape(3, self.nx)
+
+    def download_block(self, ib, ie, jb, je, kb, ke):
+        """d,u,v,w,T of the interior box [ib,ie]x[jb,je]x[kb,ke] (1-based, inclusive),
+        each (ke-kb+1, je-jb+1, ie-ib+1)."""
+        shp = (ke - kb + 1, je - jb + 1, ie - ib + 1)
+        out = [np.empty(shp) for _ in range(5)]
+        pp = (C.POINTER(C.c_double) * 5)(*[_dp(a) for a in out])
+        self._check(self.L.ocfd_gpu_download_block(self.h, ib, ie, jb, je, kb, ke, C.cast(pp, C.c_void_p)),
+                    "download_block")
+        return out
+
     @property
     def mixed(self) -> bool:
         return self.p.precision == PRECISION_MIXED

@@ -1959,6 +1959,78 @@ void orc_show_flow_msg(ocfd_oracle* o, double E0[3]) {
   for (int q = 0; q < 3; q++) E0[q] = E1[q] / N;
 }
 
+/* ana_getQ: OCFD_ANA.f90:127-171 (g[0..8] hold uk ui us vk vi vs wk wi ws) */
+void orc_ana_q(ocfd_oracle* o, double* q) {
+  double** g = o->g;
+  double** M = o->met;
+  orc_exchange_xyz(o, o->u);
+  orc_exchange_xyz(o, o->v);
+  orc_exchange_xyz(o, o->w);
+  orc_d0(o, 0, o->u, g[0]); orc_d0(o, 0, o->v, g[3]); orc_d0(o, 0, o->w, g[6]);
+  orc_d0(o, 1, o->u, g[1]); orc_d0(o, 1, o->v, g[4]); orc_d0(o, 1, o->w, g[7]);
+  orc_d0(o, 2, o->u, g[2]); orc_d0(o, 2, o->v, g[5]); orc_d0(o, 2, o->w, g[8]);
+  for (int k = 1; k <= o->nz; k++)
+    for (int j = 1; j <= o->ny; j++)
+      for (int i = 1; i <= o->nx; i++) {
+        size_t c = I3(o, i, j, k), h = IH(o, i, j, k);
+        double Akx = M[OCFD_M_AKX][h], Aky = M[OCFD_M_AKY][h], Akz = M[OCFD_M_AKZ][h];
+        double Aix = M[OCFD_M_AIX][h], Aiy = M[OCFD_M_AIY][h], Aiz = M[OCFD_M_AIZ][h];
+        double Asx = M[OCFD_M_ASX][h], Asy = M[OCFD_M_ASY][h], Asz = M[OCFD_M_ASZ][h];
+        double ux = g[0][c] * Akx + g[1][c] * Aix + g[2][c] * Asx;
+        double vx = g[3][c] * Akx + g[4][c] * Aix + g[5][c] * Asx;
+        double wx = g[6][c] * Akx + g[7][c] * Aix + g[8][c] * Asx;
+        double uy = g[0][c] * Aky + g[1][c] * Aiy + g[2][c] * Asy;
+        double vy = g[3][c] * Aky + g[4][c] * Aiy + g[5][c] * Asy;
+        double wy = g[6][c] * Aky + g[7][c] * Aiy + g[8][c] * Asy;
+        double uz = g[0][c] * Akz + g[1][c] * Aiz + g[2][c] * Asz;
+        double vz = g[3][c] * Akz + g[4][c] * Aiz + g[5][c] * Asz;
+        double wz = g[6][c] * Akz + g[7][c] * Aiz + g[8][c] * Asz;
+        q[c] = ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy;
+      }
+}
+
+/* ana_time_average: OCFD_ANA.f90:34-125, the running-mean update of the
+ * means held by the caller (5 interior arrays), K samples so far */
+void orc_ana_time_average(ocfd_oracle* o, double* mean, int K) {
+  const double* Q[5] = {o->d, o->u, o->v, o->w, o->T};
+  for (int k = 1; k <= o->nz; k++)
+    for (int j = 1; j <= o->ny; j++)
+      for (int i = 1; i <= o->nx; i++) {
+        size_t c = I3(o, i, j, k), h = IH(o, i, j, k);
+        for (int a = 0; a < 5; a++) mean[c + a * o->n] = (K * mean[c + a * o->n] + Q[a][h]) / (K + 1.0);
+      }
+}
+
+/* Ana_corner: OCFD_ANA.f90:316-384 for one rank (npx = npx0 - 1) */
+void orc_ana_corner(ocfd_oracle* o, double* out) {
+  double** M = o->met;
+  const double p00 = 1.0 / (o->p.gamma * o->p.ma * o->p.ma);
+  for (int i = 1; i <= o->nx; i++) {
+    double sx, sy;
+    if (i < o->nx) {
+      sx = M[OCFD_M_AXX][IH(o, i + 1, 1, 1)] - M[OCFD_M_AXX][IH(o, i, 1, 1)];
+      sy = M[OCFD_M_AYY][IH(o, i + 1, 1, 1)] - M[OCFD_M_AYY][IH(o, i, 1, 1)];
+    } else {
+      sx = M[OCFD_M_AXX][IH(o, o->nx, 1, 1)] - M[OCFD_M_AXX][IH(o, o->nx - 1, 1, 1)];
+      sy = M[OCFD_M_AYY][IH(o, o->nx, 1, 1)] - M[OCFD_M_AYY][IH(o, o->nx - 1, 1, 1)];
+    }
+    double tmp = 1.0 / sqrt(sx * sx + sy * sy);
+    sx = sx * tmp;
+    sy = sy * tmp;
+    double us = 0.0, Ts = 0.0, ps = 0.0;
+    for (int k = 1; k <= o->nz; k++) {
+      size_t c2 = IH(o, i, 2, k), c1 = IH(o, i, 1, k);
+      us = us + o->u[c2] * sx + o->v[c2] * sy;
+      Ts = Ts + o->T[c2];
+      ps = ps + p00 * o->d[c1] * o->T[c1];
+    }
+    double r = 1.0 / o->nz;
+    out[i - 1] = us * r;
+    out[o->nx + i - 1] = Ts * r;
+    out[2 * o->nx + i - 1] = ps * r;
+  }
+}
+
 /* ana_box: OCFD_ANA.f90:178-311 */
 void orc_ana_box(ocfd_oracle* o, double out[20]) {
   const ocfd_params* p = &o->p;

@@ -70,6 +70,9 @@ void orc_filtering(ocfd_oracle* o);
 int orc_step(ocfd_oracle* o);
 void orc_show_flow_msg(ocfd_oracle* o, double E0[3]);
 void orc_ana_box(ocfd_oracle* o, double out[20]);
+void orc_ana_q(ocfd_oracle* o, double* q);
+void orc_ana_time_average(ocfd_oracle* o, double* mean, int K);
+void orc_ana_corner(ocfd_oracle* o, double* out);
 
 /* Scheme-level entry points for the known-answer harnesses.
  * f1d has n+2*LAP values (index 1-LAP..n+LAP), hh receives n+1 faces.

@@ -64,6 +64,9 @@ def lib() -> C.CDLL:
         L.orc_flux1d.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, C.c_int, C.POINTER(C.c_int), dp]
         L.orc_char_matrices.argtypes = [C.c_double, dp, dp, dp, dp]
         L.orc_d0.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        L.orc_ana_q.argtypes = [C.c_void_p, dp]
+        L.orc_ana_time_average.argtypes = [C.c_void_p, dp, C.c_int]
+        L.orc_ana_corner.argtypes = [C.c_void_p, dp]
         L.orc_set_bc_layer.argtypes = [C.c_void_p, dp, dp, dp, C.c_int, C.c_double, dp, dp]
         _lib = L
     return _lib
@@ -197,6 +200,20 @@ class Oracle:
         e = np.zeros(3)
         lib().orc_show_flow_msg(self.h, _dp(e))
         return e
+
+    def ana_q(self):
+        q = np.empty((self.p.nz, self.p.ny, self.p.nx))
+        lib().orc_ana_q(self.h, _dp(q))
+        return q
+
+    def ana_time_average(self, mean, k_average: int):
+        """mean (5, nz, ny, nx) updated in place with the current d,u,v,w,T."""
+        lib().orc_ana_time_average(self.h, _dp(mean), k_average)
+
+    def ana_corner(self):
+        out = np.empty(3 * self.p.nx)
+        lib().orc_ana_corner(self.h, _dp(out))
+        return out.reshape(3, self.p.nx)
 
     def ana_box(self):
         e = np.zeros(20)

@@ -100,3 +100,21 @@ def test_library_accepts_and_rejects_boundary_layer_decks():
     q = p.copy()
     q.ghost_cell[2] = -2
     assert _lib.lib().ocfd_set_parameters(C.byref(q)) == _lib.OCFD_E_PARAM
+
+
+def test_analysis_deck_and_statistics_format():
+    from ocfd_b200 import analysis
+
+    deck = """ $control_opencfd
+ nx_global=16
+ ANA_Number=2
+ ANA_Para(1,1)=100, 10, 50
+ ANA_Para(1,2)=103, 5, 1, 2, 1, 3, 7
+ $end
+"""
+    e = analysis.read_analysis(deck, is_text=True)
+    assert [(c, k) for c, k, _ in e] == [(100, 10), (103, 5)]
+    assert list(e[1][2][:5]) == [1.0, 2.0, 1.0, 3.0, 7.0]
+    # '(20(E20.13E2))' of the statistics.dat row (OCFD_ANA.f90:307)
+    assert analysis.fortran_e(30.6443393820) == " 0.3064433938200E+02"
+    assert analysis.fortran_e(-1.2345e-4) == "-0.1234500000000E-03"

@@ -54,8 +54,14 @@ template <>
 struct FaceTileV<2, 1> {
   static constexpr int NP = 8, TF = 32;
 };
+#ifndef OCFD_FACE_X_VARIANT
+#define OCFD_FACE_X_VARIANT 0
+#endif
+#ifndef OCFD_FACE_YZ_VARIANT
+#define OCFD_FACE_YZ_VARIANT 0
+#endif
 template <int DIR>
-struct FaceTile : FaceTileV<DIR, 0> {};
+struct FaceTile : FaceTileV<DIR, DIR == 0 ? OCFD_FACE_X_VARIANT : OCFD_FACE_YZ_VARIANT> {};
 
 // Grid of one launch: (x, y, z) blocks for a face sweep of instance a.
 template <int DIR, int NP, int TF, typename S>
@@ -491,6 +497,58 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           const R oa[8] = {R(Omp6C::a1), R(Omp6C::a2), R(Omp6C::a3), R(Omp6C::a4),
                            R(Omp6C::a5), R(Omp6C::a6), R(Omp6C::a7), R(Omp6C::a8)};
           const R kap = R(Omp6C::kappa), ep = R(Omp6C::ep);
+#if OCFD_FEWER_DIVS
+          // production build: the projection is linear, so the linear part is
+          // L (sum_s a_s F(s)) -- the stencil sum taken in physical space and
+          // projected once -- and only the three points of the monotonicity test
+          // are projected (results move by rounding only)
+          {
+            R G[5], mid[5], vm1[5], v0[5], vp1[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+              R acc = oa[0] * W(v, 7);
+#pragma unroll
+              for (int q = 6; q >= 0; q--) acc = acc + oa[7 - q] * W(v, q);
+              G[v] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              mid[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
+              vm1[r] = proj_row(r, 0, 2);
+              v0[r] = proj_row(r, 0, 3);
+              vp1[r] = proj_row(r, 0, 4);
+              const R mp = v0[r] + minmod2((vp1[r] - v0[r]), kap * (v0[r] - vm1[r]));
+              if ((mid[r] - v0[r]) * (mid[r] - mp) >= ep) {
+                const R vm2 = proj_row(r, 0, 1), vp2 = proj_row(r, 0, 5);
+                mid[r] = omp6_limit(mid[r], vm2, vm1[r], v0[r], vp1[r], vp2, vm1[r]);
+              }
+              h0[r] = mid[r];
+            }
+          }
+          {
+            R G[5], mid[5], v0[5], v1[5], v2[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+              R acc = oa[0] * W(5 + v, 0);
+#pragma unroll
+              for (int q = 1; q <= 7; q++) acc = acc + oa[q] * W(5 + v, q);
+              G[v] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              mid[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
+              v0[r] = proj_row(r, 5, 3);
+              v1[r] = proj_row(r, 5, 4);
+              v2[r] = proj_row(r, 5, 5);
+              const R mp = v1[r] + minmod2((v0[r] - v1[r]), kap * (v1[r] - v2[r]));
+              if ((mid[r] - v1[r]) * (mid[r] - mp) >= ep) {
+                const R v3 = proj_row(r, 5, 6), vm1 = proj_row(r, 5, 2);
+                mid[r] = omp6_limit(mid[r], v3, v2[r], v1[r], v0[r], vm1, v0[r]);
+              }
+              h0[r] = h0[r] + mid[r];
+            }
+          }
+#else
           {
             R mid[5], vm1[5], v0[5], vp1[5];
 #pragma unroll
@@ -551,6 +609,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               h0[r] = h0[r] + mid[r];
             }
           }
+#endif
         } else {
           // ---- F+ projected onto the characteristic variables (:254-261), reconstructed
           {

@@ -48,6 +48,51 @@ WORKLOADS = {
 }
 
 
+# Workloads with their own grid and initial field: name -> description
+CASE_WORKLOADS = {
+    "hit512_hybrid_llf": "Decaying isotropic turbulence 512^3, Mt 0.6, Re_lambda 100, hybrid (sensor 1) "
+                         "UD7L(CD8)/WENO7/WENO5, LLF, flux-vector form, dt at CFL 0.5",
+    "cylinder_weno7_char": "Mach 6 blunt cylinder 301x401x8, body-fitted grid, isothermal wall Tw 3, Re 1e5, "
+                           "WENO7 characteristic, SW, dt 2e-5",
+}
+
+
+def make_case(workload: str, precision: str):
+    """(params, coordinates or None, interior primitives) of a workload."""
+    import math
+
+    import numpy as np
+
+    from ocfd_b200 import cases
+
+    if workload in WORKLOADS:
+        p = make_params(workload, precision)
+        return p, None, cases.tgv_prims(p)
+    if workload == "cylinder_weno7_char":
+        p = cases.cylinder_params()
+        p.precision = 1 if precision == "mixed" else 0
+        return p, cases.cylinder_grid(p.nx, p.ny, p.nz), cases.cylinder_prims(p.nx, p.ny, p.nz)
+    if workload == "hit512_hybrid_llf":
+        from ocfd_b200.solver import Solver
+
+        n, mt, ma = 512, 0.6, 1.0
+        prims = cases.hit_prims(n, mt=mt, ma=ma)
+        vmax = float(np.max(np.abs(prims[1]) + np.abs(prims[2]) + np.abs(prims[3]) + np.sqrt(prims[4]) / ma))
+        dt = 0.5 * (2.0 * math.pi / n) / vmax
+        # Re from the Taylor-scale Reynolds number of the same spectrum at 128^3 and Re = 1
+        # (Re_lambda is proportional to Re; the statistics of the k0 = 4 spectrum are
+        # resolved at both sizes)
+        q = cases.hit_params(128, re=1.0, ma=ma, dt=dt)
+        s = Solver(q)
+        s.init_mesh(*cases.hit_coords(128))
+        s.init3d(cases.hit_prims(128, mt=mt, ma=ma))
+        re = 100.0 / float(s.ana_box()[1])
+        s.close()
+        p = cases.hit_params(n, re=re, ma=ma, dt=dt, mixed=precision == "mixed")
+        return p, cases.hit_coords(n), prims
+    raise ValueError(workload)
+
+
 def make_params(workload: str, precision: str, n_override: int | None = None):
     from ocfd_b200 import cases
     from ocfd_b200.params import SCHEME
@@ -160,7 +205,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_rate(p, steps: int, warm: int = 1):
+def cpu_rate(p, steps: int, warm: int = 1, xyz=None, prims=None):
     """Oracle (CPU restatement, OpenMP over the host cores) grid-point updates per second."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle
@@ -168,8 +213,11 @@ def cpu_rate(p, steps: int, warm: int = 1):
     from ocfd_b200 import cases
 
     o = Oracle(p)
-    o.init_mesh()
-    o.init3d(cases.tgv_prims(o.p))
+    if xyz is None:
+        o.init_mesh()
+    else:
+        o.init_mesh(*xyz)
+    o.init3d(cases.tgv_prims(o.p) if prims is None else prims)
     o.step(warm)
     t0 = time.perf_counter()
     o.step(steps)
@@ -187,18 +235,38 @@ def run_reference(args):
 
     cores = multiprocessing.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    wl = WORKLOADS[args.workload]
-    nsample = min(wl[0], 128)
-    p = make_params(args.workload, "fp64", n_override=nsample)
-    rate, secs = cpu_rate(p, args.steps, warm=args.warmup)
-    ms = secs / args.steps * 1e3 * (wl[0] ** 3) / (nsample ** 3)
-    sample = (f"{args.steps} time steps of TGV {nsample}^3 (same scheme; {nsample ** 3} of the workload's "
-              f"{wl[0] ** 3} points per step) after {args.warmup} warm-up steps")
+    from ocfd_b200 import cases
+
+    if args.workload in WORKLOADS:
+        wl = WORKLOADS[args.workload]
+        desc, npts = wl[5], wl[0] ** 3
+        nsample = min(wl[0], 128)
+        p = make_params(args.workload, "fp64", n_override=nsample)
+        rate, secs = cpu_rate(p, args.steps, warm=args.warmup)
+        what = f"TGV {nsample}^3"
+    elif args.workload == "cylinder_weno7_char":
+        desc = CASE_WORKLOADS[args.workload]
+        p = cases.cylinder_params()
+        npts = p.nx * p.ny * p.nz
+        rate, secs = cpu_rate(p, args.steps, warm=args.warmup, xyz=cases.cylinder_grid(p.nx, p.ny, p.nz),
+                              prims=cases.cylinder_prims(p.nx, p.ny, p.nz))
+        what = "the cylinder case"
+    else:  # isotropic turbulence: a 128^3 sample of the same set-up
+        desc, npts = CASE_WORKLOADS[args.workload], 512 ** 3
+        p = cases.hit_params(128, re=1000.0, ma=1.0, dt=1e-3)
+        rate, secs = cpu_rate(p, args.steps, warm=args.warmup, xyz=cases.hit_coords(128),
+                              prims=cases.hit_prims(128, mt=0.6, ma=1.0))
+        what = "isotropic turbulence 128^3"
+    nsample_pts = p.nx * p.ny * p.nz
+    ms = secs / args.steps * 1e3 * npts / nsample_pts
+    sample = (f"{args.steps} time steps of {what} (same scheme; {nsample_pts} of the workload's "
+              f"{npts} points per step) after {args.warmup} warm-up steps")
+    grid = f"{p.nx}x{p.ny}x{p.nz}"
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
-        "config": {"workload": args.workload, "description": wl[5], "grid": f"{wl[0]}^3", "sample_grid": f"{nsample}^3"},
+        "config": {"workload": args.workload, "description": desc, "sample_grid": grid},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -228,11 +296,15 @@ def run_ours(args):
     from ocfd_b200 import cases
     from ocfd_b200.solver import Solver
 
-    p = make_params(args.workload, args.precision)
+    p, xyz, prims = make_case(args.workload, args.precision)
     n = p.nx * p.ny * p.nz
     s = Solver(p, device=local)
-    s.init_mesh()
-    s.init3d(cases.tgv_prims(s.p))
+    if xyz is None:
+        s.init_mesh()
+    else:
+        s.init_mesh(*xyz)
+    s.init3d(prims)
+    del prims, xyz
     stream = torch.cuda.ExternalStream(s.stream, device=local)
 
     s.step(args.warmup, sync=True)  # includes graph capture
@@ -306,7 +378,7 @@ def run_ours(args):
     line = None
     if rank == 0:
         cpu = None
-        if not args.no_cpu and world == 1:
+        if not args.no_cpu and world == 1 and args.workload in WORKLOADS:
             import multiprocessing
 
             cores = multiprocessing.cpu_count()
@@ -316,15 +388,17 @@ def run_ours(args):
             rate, secs = cpu_rate(pc, 3)
             cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                    "sample": f"3 time steps of TGV {nsample}^3 with the same scheme on the oracle ({secs:.1f} s)"}
-        wl = WORKLOADS[args.workload]
+        desc = WORKLOADS[args.workload][5] if args.workload in WORKLOADS else CASE_WORKLOADS[args.workload]
+        grid = f"{p.nx}^3" if p.nx == p.ny == p.nz else f"{p.nx}x{p.ny}x{p.nz}"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state",
-            "data": "synthetic (analytic Taylor-Green initial field)",
-            "config": {"workload": args.workload, "description": wl[5], "grid": f"{p.nx}^3", "dt": p.dt,
+            "data": ("synthetic (analytic Taylor-Green initial field)" if args.workload in WORKLOADS else
+                     "synthetic (seeded isotropic-turbulence field / analytic body-fitted grid and free stream)"),
+            "config": {"workload": args.workload, "description": desc, "grid": grid, "dt": p.dt,
                        "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state of a 256^3 grid is GBs)"},
+                       "l2": "inputs larger than L2 (the state is GBs)"},
             "clocks": clocks,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state,
                     "mode": "host-owned state: upload f + primitives, one step, download f + primitives"},
@@ -468,7 +542,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv256_omp6_char", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="tgv256_omp6_char", choices=list(WORKLOADS) + list(CASE_WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--serve", action="store_true", help="served request stream instead of the step benchmark")

@@ -16,12 +16,20 @@
 // more loads in flight, at the price of registers).  Measured best on B200 at
 // 256^3: FP64 tail 5, FP32 tail 6, FP64 viscous 4, FP32 viscous 6 (against
 // 2-3 blocks with the compiler's own register choice).
-#ifndef OCFD_VISC_MINB
-#define OCFD_VISC_MINB (sizeof(R) == 8 ? 4 : 6)
+#ifndef OCFD_VISC64_MINB
+#define OCFD_VISC64_MINB 4
 #endif
-#ifndef OCFD_TAIL_MINB
-#define OCFD_TAIL_MINB (sizeof(R) == 8 ? 5 : 6)
+#ifndef OCFD_VISC32_MINB
+#define OCFD_VISC32_MINB 6
 #endif
+#ifndef OCFD_TAIL64_MINB
+#define OCFD_TAIL64_MINB 5
+#endif
+#ifndef OCFD_TAIL32_MINB
+#define OCFD_TAIL32_MINB 6
+#endif
+#define OCFD_VISC_MINB (sizeof(R) == 8 ? OCFD_VISC64_MINB : OCFD_VISC32_MINB)
+#define OCFD_TAIL_MINB (sizeof(R) == 8 ? OCFD_TAIL64_MINB : OCFD_TAIL32_MINB)
 
 namespace ocfd {
 

@@ -297,6 +297,7 @@ int ocfd_gpu_sync(ocfd_handle* h) {
   CK(cudaStreamSynchronize(h->st));
   if (h->hstat->error == 3)
     return fail(h, OCFD_E_NEGT, "Number of Negative Temperature Points >  Limit, STOP !");
+  if (h->hstat->error == 4) return fail(h, OCFD_E_TIMEOUT, "a bounded device wait gave up (tile copy)");
   return OCFD_OK;
 }
 
@@ -652,6 +653,7 @@ static FaceArgs<S> face_args(ocfd_handle* h, int d) {
   a.fbeg = h->ph.periodic[d] ? 1 : 0;
   a.fend = g.len(d);
   a.split = h->p.flux_splitting;
+  a.err = &h->dstat->error;
   return a;
 }
 

@@ -195,6 +195,7 @@ struct FaceArgs {
   long long fs;      // per-variable stride of hh
   int fbeg, fend;    // faces computed: fbeg..fend
   int split;         // 1 SW, 2 LLF
+  int* err;          // DevStatus::error of the instance (bounded waits record 4 there)
   Phys ph;
 };
 
@@ -202,7 +203,7 @@ struct FaceArgs {
 struct DevStatus {
   int negt_count;     // points with T <= 0 found by the current primitive recovery
   int negt_list[16];  // their haloed linear indices (first 16)
-  int error;          // sticky error: 3 = negative-T limit exceeded
+  int error;          // sticky error: 3 = negative-T limit exceeded, 4 = a bounded device wait gave up
   int negt_last;      // points repaired in the last stage
   int negt_total;     // points repaired since creation
   int pad[12];

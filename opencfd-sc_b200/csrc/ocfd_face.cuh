@@ -22,6 +22,7 @@
 #include "ocfd_device.cuh"
 #include "ocfd_kernels.h"
 #include "ocfd_schemes.cuh"
+#include "ocfd_tma.cuh"
 
 namespace ocfd {
 
@@ -217,8 +218,12 @@ struct Stencil<SCH_WENO5> {
 // the boundary-closure paths are compiled out.
 // The body of one block; (bx, by, bz) are its block coordinates within the
 // instance's own launch grid.
-template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S>
-__device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, const int by, const int bz, R* sm) {
+// TMA: the eight input arrays were staged in shared memory by the caller
+// (tile: TmaBox slots of d, u, v, w, T, A1, A2, A3; toff: offset of the first
+// stencil point / pencil in the tile's innermost dimension).
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S, bool TMA = false>
+__device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, const int by, const int bz, R* sm,
+                                          const S* tile = nullptr, int toff = 0) {
   constexpr int LT = TF + 7;
   // shared memory: 10 split-flux arrays (+7 face-state arrays for CHAR)
   auto SI = [](int var, int l, int p) -> int { return var * (NP * LT) + (DIR == 0 ? p * LT + l : l * NP + p); };
@@ -271,7 +276,19 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
     const int gl = g0 - 3 + l;  // point index along DIR
     ok = ok && gl <= nn + LAP;
     R d = R(1), u = R(1), v = R(1), w = R(1), T = R(1), A1 = R(1), A2 = R(1), A3 = R(1);
-    if (ok) {
+    if (ok && TMA) {
+      using B = TmaBox<DIR, NP, TF, S>;
+      const int e = DIR == 0 ? p * B::BX + l + toff : l * B::BX + p + toff;
+      d = R(tile[e]);
+      u = R(tile[B::SLOT_ELEMS + e]);
+      v = R(tile[2 * B::SLOT_ELEMS + e]);
+      w = R(tile[3 * B::SLOT_ELEMS + e]);
+      T = R(tile[4 * B::SLOT_ELEMS + e]);
+      const int m0 = 13 + 3 * DIR;
+      A1 = ((ph.metzero >> m0) & 1u) ? R(0) : R(tile[5 * B::SLOT_ELEMS + e]);
+      A2 = ((ph.metzero >> (m0 + 1)) & 1u) ? R(0) : R(tile[6 * B::SLOT_ELEMS + e]);
+      A3 = ((ph.metzero >> (m0 + 2)) & 1u) ? R(0) : R(tile[7 * B::SLOT_ELEMS + e]);
+    } else if (ok) {
       long long h = G.ih(i, j, k) + (long long)gl * hs;
       d = R(__ldg(a.d + h));
       u = R(__ldg(a.u + h));
@@ -686,6 +703,58 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<Fac
       batch_args(b, q, &sa), bx, by, bz, reinterpret_cast<R*>(smem_raw));
 }
 
+// Single-instance sweep of a periodic direction with the input tiles staged by
+// TMA (the arithmetic is that of k_face).
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+__global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
+  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+  using B = TmaBox<DIR, NP, TF, S>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  // TMA destinations start on 128-byte boundaries (128 bytes of the launch's
+  // dynamic shared memory are reserved for this rounding)
+  unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127u)) & 127u);
+  S* tile = reinterpret_cast<S*>(base);
+  R* sm = reinterpret_cast<R*>(base + 8 * B::SLOT);
+  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+  const int g0 = a.fbeg + (DIR == 0 ? bx : by) * TF;  // first face; its stencil starts at g0 - 3
+  const int pbase = (DIR == 0 ? by : bx) * NP;
+  // haloed (0-based) coordinates of the tile's first element: index + LAP - 1
+  const int x0 = DIR == 0 ? g0 : pbase + 4;
+  const int toff = x0 % B::A;
+  const int c0 = x0 - toff;
+  const int c1 = DIR == 0 ? pbase + 4 : (DIR == 1 ? g0 : bz + 4);
+  const int c2 = DIR == 2 ? g0 : bz + 4;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int m0 = 13 + 3 * DIR;
+    bool need[8];
+    uint32_t bytes = 0;
+    for (int q = 0; q < 8; q++) {
+      need[q] = q < 5 || !((a.ph.metzero >> (m0 + q - 5)) & 1u);
+      if (need[q]) bytes += B::BYTES;
+    }
+    mbar_arrive_expect_tx(&bar, bytes);
+    for (int q = 0; q < 8; q++)
+      if (need[q]) tma_load_3d(tile + q * B::SLOT_ELEMS, &tm.m[q], c0, c1, c2, &bar);
+  }
+  // bounded wait (about a second); a block that gives up records the error and
+  // waits once more, again bounded, for its copies before leaving
+  bool done = mbar_wait_bounded(&bar, 0, 1u << 20);
+  if (__syncthreads_or(!done)) {
+    if (threadIdx.x == 0) {
+      atomicExch(a.err, 4);
+      mbar_wait_bounded(&bar, 0, 1u << 20);
+    }
+    return;
+  }
+  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true>(a, bx, by, bz, sm, tile, toff);
+}
+
 template <int DIR, bool CHAR, int NP, int TF, typename R>
 constexpr size_t face_smem() {
   return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R);  // split fluxes (+ face state)
@@ -746,9 +815,58 @@ dim3 face_batch_dims(int dir, int variant, const FaceArgs<S>& a) {
   return variant ? face_grid<2, 8, 32>(a) : face_grid<2, 16, 16>(a);
 }
 
+// ---- TMA path: tensor maps of the sweep's eight input arrays
+bool face_tma_enabled();
+bool encode_tile_map(CUtensorMap* map, const void* base, bool f64, const Grid& g, int bx, int by, int bz);
+
+template <typename S>
+inline bool tma_strides_ok(const Grid& g) {
+  return ((long long)g.nxh * sizeof(S)) % 16 == 0 && ((long long)g.nxh * g.nyh * sizeof(S)) % 16 == 0;
+}
+
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
+  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+  using B = TmaBox<DIR, NP, TF, S>;
+  constexpr size_t smem = 128 + 8 * (size_t)B::SLOT + face_smem<DIR, CHAR, NP, TF, R>();
+  auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S>;
+  if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  FaceTmaMaps tm;
+  const S* arr[8] = {a.d, a.u, a.v, a.w, a.T, a.A1, a.A2, a.A3};
+  for (int q = 0; q < 8; q++)
+    if (!encode_tile_map(&tm.m[q], arr[q], sizeof(S) == 8, a.g, B::BX, B::BY, B::BZ)) return cudaErrorInvalidValue;
+  kern<<<face_grid<DIR, NP, TF>(a), NP * TF, smem, st>>>(a, tm);
+  return cudaGetLastError();
+}
+
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st) {
   const bool allin = a.ph.periodic[dir] != 0;
+  // TMA staging for the FP64 sweeps (measured 1-3% faster at 256^3); the FP32
+  // sweeps, four blocks per SM, are as fast or faster with plain loads
+  if constexpr (sizeof(S) == 8)
+  if (allin && (a.g.n == 0 || (face_tma_enabled() && tma_strides_ok<S>(a.g)))) {
+    // set-up (empty grid) registers both kernels; launches take the TMA path
+#define OCFD_FACE_TMA_CASE(D, C, SC)                                                        \
+    if (dir == D && chr == C && scheme == SC) {                                               \
+      cudaError_t e = launch_face_tma_t<D, C, SC, R, S>(a, st);                               \
+      if (a.g.n != 0 || e != cudaSuccess) return e;                                           \
+    }
+#define OCFD_FACE_TMA_SCHEMES(D, C) \
+    OCFD_FACE_TMA_CASE(D, C, SCH_WENO5) \
+    OCFD_FACE_TMA_CASE(D, C, SCH_WENO7) \
+    OCFD_FACE_TMA_CASE(D, C, SCH_OMP6)  \
+    OCFD_FACE_TMA_CASE(D, C, SCH_UD7L)  \
+    OCFD_FACE_TMA_CASE(D, C, SCH_HYBRID)
+    OCFD_FACE_TMA_SCHEMES(0, false)
+    OCFD_FACE_TMA_SCHEMES(1, false)
+    OCFD_FACE_TMA_SCHEMES(2, false)
+    OCFD_FACE_TMA_SCHEMES(0, true)
+    OCFD_FACE_TMA_SCHEMES(1, true)
+    OCFD_FACE_TMA_SCHEMES(2, true)
+#undef OCFD_FACE_TMA_SCHEMES
+#undef OCFD_FACE_TMA_CASE
+  }
 #define OCFD_FACE_CASE(D, C, SC)                                                    \
   if (dir == D && chr == C && scheme == SC)                                         \
     return allin ? launch_face_t<D, C, SC, true, R, S>(a, st) : launch_face_t<D, C, SC, false, R, S>(a, st);

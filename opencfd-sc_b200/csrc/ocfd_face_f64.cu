@@ -1,7 +1,55 @@
 // FP64 instantiations of the face-flux kernels (ocfd_face.cuh).
 #include "ocfd_face.cuh"
 
+#include <cstdlib>
+
 namespace ocfd {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*TileEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static TileEncodeFn tile_encoder() {
+  static TileEncodeFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<TileEncodeFn>(f);
+  }
+  return fn;
+}
+
+// TMA staging of the periodic face sweeps: on unless OCFD_FACE_TMA=0 (or the
+// driver offers no tensor-map encoder).
+bool face_tma_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("OCFD_FACE_TMA");
+    on = (e && e[0] == '0') ? 0 : (tile_encoder() != nullptr ? 1 : 0);
+  }
+  return on == 1;
+}
+
+// Tiled 3-D map of a haloed (nxh, nyh, nzh) array, box (bx, by, bz); tiles
+// reaching past the array read zeros.
+bool encode_tile_map(CUtensorMap* map, const void* base, bool f64, const Grid& g, int bx, int by, int bz) {
+  TileEncodeFn fn = tile_encoder();
+  if (!fn) return false;
+  const cuuint64_t es = f64 ? 8 : 4;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.nxh, (cuuint64_t)g.nyh, (cuuint64_t)g.nzh};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.nxh * es, (cuuint64_t)g.nxh * g.nyh * es};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base),
+            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template cudaError_t launch_face<double, double>(int, bool, int, const FaceArgs<double>&, cudaStream_t);
 
 // A FaceArgs with an empty grid asks launch_face_t to set the kernel's

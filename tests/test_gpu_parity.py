@@ -11,6 +11,8 @@ Two builds of the library run every case:
 The sensor-2 hybrid case uses a parallel reduction for the domain mean and is
 compared with tolerance in both builds.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -261,3 +263,29 @@ def test_metric_zero_mask_box_and_curvilinear():
     for m in (3, 4, 6, 7, 11, 13, 14, 16, 17, 21):
         assert not (s.metric_zero_mask() >> m) & 1, m
     s.close()
+
+
+def test_tma_staged_sweeps_equal_plain_loads(tmp_path):
+    """The FP64 periodic face sweeps stage their inputs with TMA; with the
+    staging switched off (OCFD_FACE_TMA=0, read once per process) the results
+    are the same bits."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, numpy as np; sys.path[:0] = sys.argv[2:];"
+        "from ocfd_testlib import tgv_case; from ocfd_b200.solver import Solver;"
+        "from ocfd_b200.params import SCHEME_OMP6;"
+        "p, _, pr = tgv_case(scheme=SCHEME_OMP6, character=1, n=(32, 24, 20));"
+        "s = Solver(p); s.init_mesh(); s.init3d(pr); s.step(3); np.save(sys.argv[1], s.download_f())"
+    )
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    paths = [here, os.path.join(root, "oracle"), os.path.join(root, "opencfd-sc_b200")]
+    outs = []
+    for flag in ("1", "0"):
+        out = str(tmp_path / f"f{flag}.npy")
+        subprocess.run([sys.executable, "-c", code, out] + paths, check=True,
+                       env=dict(os.environ, OCFD_FACE_TMA=flag))
+        outs.append(np.load(out))
+    np.testing.assert_array_equal(outs[0], outs[1])

@@ -227,6 +227,42 @@ def cpu_rate(p, steps: int, warm: int = 1, xyz=None, prims=None):
     return n * steps / dt / 1e9, dt
 
 
+def data_kind(workload: str) -> str:
+    if workload in WORKLOADS:
+        return "synthetic (analytic Taylor-Green initial field)"
+    if workload == "cylinder_weno7_char":
+        return "synthetic (analytic body-fitted grid and uniform free stream)"
+    return "synthetic (seeded isotropic-turbulence field)"
+
+
+def cpu_sample(workload: str, steps: int, warm: int):
+    """The oracle on a bounded sample of `workload`: (rate, seconds, sample name,
+    sample params, workload description, workload points per step)."""
+    from ocfd_b200 import cases
+
+    if workload in WORKLOADS:
+        wl = WORKLOADS[workload]
+        desc, npts = wl[5], wl[0] ** 3
+        nsample = min(wl[0], 128)
+        p = make_params(workload, "fp64", n_override=nsample)
+        rate, secs = cpu_rate(p, steps, warm=warm)
+        what = f"TGV {nsample}^3"
+    elif workload == "cylinder_weno7_char":
+        desc = CASE_WORKLOADS[workload]
+        p = cases.cylinder_params()
+        npts = p.nx * p.ny * p.nz
+        rate, secs = cpu_rate(p, steps, warm=warm, xyz=cases.cylinder_grid(p.nx, p.ny, p.nz),
+                              prims=cases.cylinder_prims(p.nx, p.ny, p.nz))
+        what = "the cylinder case"
+    else:  # isotropic turbulence: a 128^3 sample of the same set-up
+        desc, npts = CASE_WORKLOADS[workload], 512 ** 3
+        p = cases.hit_params(128, re=1000.0, ma=1.0, dt=1e-3)
+        rate, secs = cpu_rate(p, steps, warm=warm, xyz=cases.hit_coords(128),
+                              prims=cases.hit_prims(128, mt=0.6, ma=1.0))
+        what = "isotropic turbulence 128^3"
+    return rate, secs, what, p, desc, npts
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -235,28 +271,7 @@ def run_reference(args):
 
     cores = multiprocessing.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    from ocfd_b200 import cases
-
-    if args.workload in WORKLOADS:
-        wl = WORKLOADS[args.workload]
-        desc, npts = wl[5], wl[0] ** 3
-        nsample = min(wl[0], 128)
-        p = make_params(args.workload, "fp64", n_override=nsample)
-        rate, secs = cpu_rate(p, args.steps, warm=args.warmup)
-        what = f"TGV {nsample}^3"
-    elif args.workload == "cylinder_weno7_char":
-        desc = CASE_WORKLOADS[args.workload]
-        p = cases.cylinder_params()
-        npts = p.nx * p.ny * p.nz
-        rate, secs = cpu_rate(p, args.steps, warm=args.warmup, xyz=cases.cylinder_grid(p.nx, p.ny, p.nz),
-                              prims=cases.cylinder_prims(p.nx, p.ny, p.nz))
-        what = "the cylinder case"
-    else:  # isotropic turbulence: a 128^3 sample of the same set-up
-        desc, npts = CASE_WORKLOADS[args.workload], 512 ** 3
-        p = cases.hit_params(128, re=1000.0, ma=1.0, dt=1e-3)
-        rate, secs = cpu_rate(p, args.steps, warm=args.warmup, xyz=cases.hit_coords(128),
-                              prims=cases.hit_prims(128, mt=0.6, ma=1.0))
-        what = "isotropic turbulence 128^3"
+    rate, secs, what, p, desc, npts = cpu_sample(args.workload, args.steps, args.warmup)
     nsample_pts = p.nx * p.ny * p.nz
     ms = secs / args.steps * 1e3 * npts / nsample_pts
     sample = (f"{args.steps} time steps of {what} (same scheme; {nsample_pts} of the workload's "
@@ -265,7 +280,7 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
+        "dtype": "f64", "data": data_kind(args.workload),
         "config": {"workload": args.workload, "description": desc, "sample_grid": grid},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                          "sample": sample},
@@ -378,24 +393,24 @@ def run_ours(args):
     line = None
     if rank == 0:
         cpu = None
-        if not args.no_cpu and world == 1 and args.workload in WORKLOADS:
+        if not args.no_cpu and world == 1:
             import multiprocessing
 
             cores = multiprocessing.cpu_count()
             os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-            nsample = min(p.nx, 128)
-            pc = make_params(args.workload, "fp64", n_override=nsample)
-            rate, secs = cpu_rate(pc, 3)
+            # about 10 s of the host's cores: 2 warm-up steps, then enough steps
+            rate, secs, what, _, _, _ = cpu_sample(args.workload, 2, 1)
+            nst = int(min(40, max(3, 10.0 / max(secs / 2, 1e-3))))
+            rate, secs, what, _, _, _ = cpu_sample(args.workload, nst, 1)
             cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                   "sample": f"3 time steps of TGV {nsample}^3 with the same scheme on the oracle ({secs:.1f} s)"}
+                   "sample": f"{nst} time steps of {what} with the same scheme on the oracle ({secs:.1f} s)"}
         desc = WORKLOADS[args.workload][5] if args.workload in WORKLOADS else CASE_WORKLOADS[args.workload]
         grid = f"{p.nx}^3" if p.nx == p.ny == p.nz else f"{p.nx}x{p.ny}x{p.nz}"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state",
-            "data": ("synthetic (analytic Taylor-Green initial field)" if args.workload in WORKLOADS else
-                     "synthetic (seeded isotropic-turbulence field / analytic body-fitted grid and free stream)"),
+            "data": data_kind(args.workload),
             "config": {"workload": args.workload, "description": desc, "grid": grid, "dt": p.dt,
                        "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (the state is GBs)"},

@@ -213,6 +213,116 @@ struct Stencil<SCH_WENO5> {
   static constexpr int PLO = -2, PHI = 2, MLO = -1, MHI = 3;
 };
 
+// Block-wide queue of OMP6 limiter evaluations (characteristic form,
+// production build).  The monotonicity test of the ten characteristic
+// components of a face is cheap; the limiter that a failed test calls is not,
+// and the faces that need it are scattered, so a warp running it for one lane
+// would idle the other 31.  Instead each flagged (face, component) is queued
+// in shared memory -- its unlimited value and a tag (stencil window, component,
+// side) -- and the whole block evaluates the queue, one entry per thread:
+// eigenvector row, the five projected stencil values and the limiter.  The
+// capacity is ten entries per face, so the queue never overflows.
+struct LimQueue {
+  static constexpr int CAP = 2560;
+  template <typename R>
+  static constexpr size_t bytes() {
+    return ((size_t)CAP * sizeof(R) + (CAP + 1) * sizeof(int) + 15) / 16 * 16;
+  }
+};
+
+// Arithmetic with explicit rounding: never contracted or reassociated, so an
+// expression written with these gives the same bits wherever it is inlined.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xrcp(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float xrcp(float a) { return __frcp_rn(a); }
+
+// One queued limiter evaluation (OCFD_inviscous_character.f90:205-248 for the
+// face state and row r of the left eigenvector matrix, :256-270 for the
+// projection, OCFD_Schemes_1.f90:212-224 for the limiter): the face whose
+// stencil window starts at wb, component r, F+ points -2..2 (window 1..5) or
+// F- mirrored (window 6..2), unlimited value mid.  Written in explicitly
+// rounded operations, so that every kernel that inlines it produces the same
+// bits.
+template <typename R, int VS, int QS>
+__device__ __forceinline__ R lim_eval(const R* wb, int r, int minus, R mid, R gm1) {
+  auto mean = [&](int var) { return xmul(xadd(wb[var * VS + 3 * QS], wb[var * VS + 4 * QS]), R(0.5)); };
+  const R u1 = mean(10), v1 = mean(11), w1 = mean(12), c1 = mean(13), a1 = mean(14), a2 = mean(15), a3 = mean(16);
+  const R rs = rsqrt(xfma(a3, a3, xfma(a2, a2, xmul(a1, a1))));
+  const R n1 = xmul(a1, rs), n2 = xmul(a2, rs), n3 = xmul(a3, rs);
+  R l1, l2, l3;
+  if (fabs(n3) <= fabs(n2)) {
+    const R rl = rsqrt(xfma(n2, n2, xmul(n1, n1)));
+    l1 = -xmul(n2, rl);
+    l2 = xmul(n1, rl);
+    l3 = R(0);
+  } else {
+    const R rl = rsqrt(xfma(n3, n3, xmul(n1, n1)));
+    l1 = -xmul(n3, rl);
+    l3 = xmul(n1, rl);
+    l2 = R(0);
+  }
+  R c[5];
+  if (r == 1) {
+    c[0] = -xfma(w1, l3, xfma(v1, l2, xmul(u1, l1)));
+    c[1] = l1;
+    c[2] = l2;
+    c[3] = l3;
+    c[4] = R(0);
+  } else if (r == 2) {
+    const R m1 = xfma(n2, l3, -xmul(n3, l2)), m2 = xfma(n3, l1, -xmul(n1, l3)), m3 = xfma(n1, l2, -xmul(n2, l1));
+    c[0] = -xfma(w1, m3, xfma(v1, m2, xmul(u1, m1)));
+    c[1] = m1;
+    c[2] = m2;
+    c[3] = m3;
+    c[4] = R(0);
+  } else {
+    const R rc = xrcp(c1);
+    const R KK = xmul(gm1, xmul(rc, rc));
+    const R V2 = xmul(xfma(w1, w1, xfma(v1, v1, xmul(u1, u1))), R(0.5));
+    if (r == 0) {
+      c[0] = xfma(-KK, V2, R(1));
+      c[1] = xmul(KK, u1);
+      c[2] = xmul(KK, v1);
+      c[3] = xmul(KK, w1);
+      c[4] = -KK;
+    } else {
+      const R KK1 = xmul(KK, R(0.5)), X1 = xmul(R(0.5), rc);
+      const R sX = r == 3 ? X1 : -X1;
+      const R un = xfma(w1, n3, xfma(v1, n2, xmul(u1, n1)));
+      c[0] = xfma(sX, un, xmul(KK1, V2));
+      c[1] = xfma(-sX, n1, -xmul(KK1, u1));
+      c[2] = xfma(-sX, n2, -xmul(KK1, v1));
+      c[3] = xfma(-sX, n3, -xmul(KK1, w1));
+      c[4] = KK1;
+    }
+  }
+  const R* w0 = wb + (minus ? 5 * VS + 6 * QS : QS);
+  const int qs = minus ? -QS : QS;
+  R x[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const R* wq = w0 + k * qs;
+    x[k] = xfma(c[4], wq[4 * VS], xfma(c[3], wq[3 * VS], xfma(c[2], wq[2 * VS], xfma(c[1], wq[VS], xmul(c[0], wq[0])))));
+  }
+  const R s0 = x[2], s1 = x[3], vlc = minus ? x[3] : x[1];  // v(0), v(1), the lc reference
+  const R kappa = R(Omp6C::kappa);
+  const R d1 = xfma(R(-2), x[1], xadd(x[0], s0));
+  const R d2 = xfma(R(-2), s0, xadd(x[1], s1));
+  const R d3 = xfma(R(-2), s1, xadd(s0, x[4]));
+  const R ul = xfma(kappa, xadd(s0, -x[1]), s0);
+  const R md = xfma(R(-0.5), minmod4(xfma(R(4), d2, -d3), xfma(R(4), d3, -d2), d2, d3), xmul(R(0.5), xadd(s0, s1)));
+  const R lc = xfma(R(Omp6C::kappa / 3.0), minmod4(xfma(R(4), d1, -d2), xfma(R(4), d2, -d1), d2, d1),
+                    xfma(R(0.5), xadd(s0, -vlc), s0));
+  const R fmin = rmax(rmin(rmin(s0, s1), md), rmin(rmin(s0, ul), lc));
+  const R fmax = rmin(rmax(rmax(s0, s1), md), rmax(rmax(s0, ul), lc));
+  return xadd(mid, minmod2(xadd(fmax, -mid), xadd(fmin, -mid)));
+}
+
 // ---------------------------------------------------------------------------
 // ALLIN: every face of the launch is an interior face (periodic direction), so
 // the boundary-closure paths are compiled out.
@@ -260,6 +370,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   };
   const long long hs = G.hstride(DIR);
   const R gam = R(ph.gamma), ma = R(ph.ma);
+  // deferred OMP6 limiter (characteristic form, production build): queue after
+  // the 17 staged arrays -- CAP unlimited values, CAP tags (window offset * 16 +
+  // component * 2 + side), the entry count
+  constexpr bool DEFER = CHAR && SCHEME == SCH_OMP6 && OCFD_FEWER_DIVS;
+  constexpr int JC = LimQueue::CAP;
+  static_assert(!DEFER || NP * TF == 256, "the deferred limiter assumes one face per thread");
+  R* const jv = sm + 17 * NP * LT;
+  int* const jtag = reinterpret_cast<int*>(jv + JC);
+  int* const jn = jtag + JC;
+  if (DEFER && threadIdx.x == 0) *jn = 0;
 
   // ---- phase 1: split fluxes of the tile's points into shared memory
   for (int t = threadIdx.x; t < NP * LT; t += blockDim.x) {
@@ -333,6 +453,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   R* out = reinterpret_cast<R*>(a.hh);
   // window element (var, stencil offset s) of this thread's face at wb[var*VS + (s+3)*QS]
   constexpr int VS = NP * LT, QS = DIR == 0 ? 1 : NP;
+  // state of a face whose limiter evaluations are queued: the F+ / F- parts of
+  // the characteristic flux, the flags of the queued components and their first
+  // queue entry, the face's output offset and the basis of the back projection
+  R dP[5], dM[5];
+  unsigned dfl = 0;
+  int djb = 0;
+  bool dpend = false;
+  long long dfo = 0;
+  R bu = R(0), bv = R(0), bw = R(0), bc = R(0), bn1 = R(0), bn2 = R(0), bn3 = R(0), bl1 = R(0), bl2 = R(0),
+    bl3 = R(0);
 
   for (int t = threadIdx.x; t < NP * TF; t += blockDim.x) {
     int f, p;
@@ -518,9 +648,10 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           // production build: the projection is linear, so the linear part is
           // L (sum_s a_s F(s)) -- the stencil sum taken in physical space and
           // projected once -- and only the three points of the monotonicity test
-          // are projected (results move by rounding only)
+          // are projected (results move by rounding only).  Components that fail
+          // the test are queued for the block-wide limiter pass below.
           {
-            R G[5], mid[5], vm1[5], v0[5], vp1[5];
+            R G[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
               R acc = oa[0] * W(v, 7);
@@ -530,20 +661,14 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             }
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              mid[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
-              vm1[r] = proj_row(r, 0, 2);
-              v0[r] = proj_row(r, 0, 3);
-              vp1[r] = proj_row(r, 0, 4);
-              const R mp = v0[r] + minmod2((vp1[r] - v0[r]), kap * (v0[r] - vm1[r]));
-              if ((mid[r] - v0[r]) * (mid[r] - mp) >= ep) {
-                const R vm2 = proj_row(r, 0, 1), vp2 = proj_row(r, 0, 5);
-                mid[r] = omp6_limit(mid[r], vm2, vm1[r], v0[r], vp1[r], vp2, vm1[r]);
-              }
-              h0[r] = mid[r];
+              dP[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
+              const R vm1 = proj_row(r, 0, 2), v0 = proj_row(r, 0, 3), vp1 = proj_row(r, 0, 4);
+              const R mp = v0 + minmod2((vp1 - v0), kap * (v0 - vm1));
+              dfl |= ((dP[r] - v0) * (dP[r] - mp) >= ep ? 1u : 0u) << r;
             }
           }
           {
-            R G[5], mid[5], v0[5], v1[5], v2[5];
+            R G[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
               R acc = oa[0] * W(5 + v, 0);
@@ -553,18 +678,42 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             }
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              mid[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
-              v0[r] = proj_row(r, 5, 3);
-              v1[r] = proj_row(r, 5, 4);
-              v2[r] = proj_row(r, 5, 5);
-              const R mp = v1[r] + minmod2((v0[r] - v1[r]), kap * (v1[r] - v2[r]));
-              if ((mid[r] - v1[r]) * (mid[r] - mp) >= ep) {
-                const R v3 = proj_row(r, 5, 6), vm1 = proj_row(r, 5, 2);
-                mid[r] = omp6_limit(mid[r], v3, v2[r], v1[r], v0[r], vm1, v0[r]);
-              }
-              h0[r] = h0[r] + mid[r];
+              dM[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
+              const R v0 = proj_row(r, 5, 3), v1 = proj_row(r, 5, 4), v2 = proj_row(r, 5, 5);
+              const R mp = v1 + minmod2((v0 - v1), kap * (v1 - v2));
+              dfl |= ((dM[r] - v1) * (dM[r] - mp) >= ep ? 1u : 0u) << (5 + r);
             }
           }
+          if (dfl) {
+            // queue entries djb, djb+1, ... in the order (r, F+ then F-)
+            djb = atomicAdd(jn, __popc(dfl));
+            const int woff = (int)(wb - sm);
+            int e = djb;
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+#pragma unroll
+              for (int side = 0; side < 2; side++) {
+                if ((dfl >> (5 * side + r)) & 1u) {
+                  jv[e] = side ? dM[r] : dP[r];
+                  jtag[e] = 16 * woff + 2 * r + side;
+                  e++;
+                }
+              }
+            }
+          }
+          dpend = true;
+          dfo = fo;
+          bu = u1;
+          bv = v1;
+          bw = w1;
+          bc = c1;
+          bn1 = n1;
+          bn2 = n2;
+          bn3 = n3;
+          bl1 = l1;
+          bl2 = l2;
+          bl3 = l3;
+          continue;
 #else
           {
             R mid[5], vm1[5], v0[5], vp1[5];
@@ -673,6 +822,44 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #pragma unroll
     for (int m = 0; m < 5; m++) out[fo + (long long)m * a.fs] = hh[m];
   }
+  if constexpr (DEFER) {
+    __syncthreads();
+    const int nj = min(*jn, JC);
+    const R gm1 = R(ph.gamma) - R(1);
+    for (int e = threadIdx.x; e < nj; e += blockDim.x) {
+      const int tag = jtag[e];
+      jv[e] = lim_eval<R, VS, QS>(sm + (tag >> 4), (tag >> 1) & 7, tag & 1, jv[e], gm1);
+    }
+    __syncthreads();
+    if (dpend) {
+      if (dfl) {
+        int e = djb;
+#pragma unroll
+        for (int r = 0; r < 5; r++) {
+          if ((dfl >> r) & 1u) dP[r] = jv[e++];
+          if ((dfl >> (5 + r)) & 1u) dM[r] = jv[e++];
+        }
+      }
+      // back to physical space, hh = R h0 (OCFD_inviscous_character.f90:284-288)
+      R h0[5];
+#pragma unroll
+      for (int r = 0; r < 5; r++) h0[r] = dP[r] + dM[r];
+      const R m1 = bn2 * bl3 - bn3 * bl2, m2 = bn3 * bl1 - bn1 * bl3, m3 = bn1 * bl2 - bn2 * bl1;
+      const R un = bu * bn1 + bv * bn2 + bw * bn3;
+      const R ul = bu * bl1 + bv * bl2 + bw * bl3;
+      const R um = bu * m1 + bv * m2 + bw * m3;
+      const R V2 = (bu * bu + bv * bv + bw * bw) * R(0.5);
+      const R H = V2 + bc * bc * R(ph.inv_gm1);
+      R hh[5];
+      hh[0] = h0[0] + h0[3] + h0[4];
+      hh[1] = bu * h0[0] + bl1 * h0[1] + m1 * h0[2] + (bu - bc * bn1) * h0[3] + (bu + bc * bn1) * h0[4];
+      hh[2] = bv * h0[0] + bl2 * h0[1] + m2 * h0[2] + (bv - bc * bn2) * h0[3] + (bv + bc * bn2) * h0[4];
+      hh[3] = bw * h0[0] + bl3 * h0[1] + m3 * h0[2] + (bw - bc * bn3) * h0[3] + (bw + bc * bn3) * h0[4];
+      hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - bc * un) * h0[3] + (H + bc * un) * h0[4];
+#pragma unroll
+      for (int m = 0; m < 5; m++) out[dfo + (long long)m * a.fs] = hh[m];
+    }
+  }
 }
 
 // Minimum resident blocks per SM.  FP64: two (<= 128 registers) measured
@@ -757,7 +944,8 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_tma(FaceArgs<S> a,
 
 template <int DIR, bool CHAR, int NP, int TF, typename R>
 constexpr size_t face_smem() {
-  return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R);  // split fluxes (+ face state)
+  // split fluxes (+ face state and the limiter queue)
+  return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R) + (CHAR ? LimQueue::bytes<R>() : 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -218,17 +218,28 @@ __device__ __forceinline__ R weno7M(const R* v) {
 }
 
 // minmod2 / minmod4: OCFD_Schemes.f90:274-289
-template <typename R>
-__device__ __forceinline__ R minmod2(R x1, R x2) {
-  return R(0.5) * (sign1(x1) + sign1(x2)) * rmin(fabs(x1), fabs(x2));
+// minmod2 = 0.5*(sign(1,x1) + sign(1,x2)) * min(|x1|, |x2|): the sign factor is
+// +-1 when the sign bits agree and 0 otherwise, so for finite arguments the
+// value is min(|x1|,|x2|) with the sign of x1, or +0 -- the same bits, one
+// comparison instead of three floating-point operations.
+__device__ __forceinline__ bool sign_bits_differ(double a, double b) {
+  return (__double_as_longlong(a) ^ __double_as_longlong(b)) < 0;
+}
+__device__ __forceinline__ bool sign_bits_differ(float a, float b) {
+  return (__float_as_int(a) ^ __float_as_int(b)) < 0;
 }
 template <typename R>
+__device__ __forceinline__ R minmod2(R x1, R x2) {
+  return sign_bits_differ(x1, x2) ? R(0) : copysign(rmin(fabs(x1), fabs(x2)), x1);
+}
+// minmod4 = 0.5*(s1+s2) * |0.5*(s1+s3)| * |0.5*(s1+s4)| * min|x| (s = sign(1,x)):
+// +0 when the sign bits of x1 and x2 differ; otherwise the product carries the
+// sign of x1 and is min|x| when x3 and x4 share that sign bit, else a zero.
+template <typename R>
 __device__ __forceinline__ R minmod4(R x1, R x2, R x3, R x4) {
-  R r = R(0.5) * (sign1(x1) + sign1(x2));
-  r = r * fabs(R(0.5) * (sign1(x1) + sign1(x3)));
-  r = r * fabs(R(0.5) * (sign1(x1) + sign1(x4)));
-  r = r * rmin(rmin(rmin(fabs(x1), fabs(x2)), fabs(x3)), fabs(x4));
-  return r;
+  if (sign_bits_differ(x1, x2)) return R(0);
+  const R m = rmin(rmin(rmin(fabs(x1), fabs(x2)), fabs(x3)), fabs(x4));
+  return copysign((sign_bits_differ(x1, x3) || sign_bits_differ(x1, x4)) ? R(0) : m, x1);
 }
 
 // OMP6 (optimized 6th-order monotonicity-preserving) coefficients,
@@ -255,7 +266,7 @@ struct Omp6C {
 // vlc is the value subtracted in the lc term: v(-1) in hh_OMP6P
 // (OCFD_Schemes_1.f90:219) but v(0) -- not the mirror v(2) -- in hh_OMP6M (:253).
 template <typename R>
-__device__ __noinline__ R omp6_limit(R mid_nf, R vm2, R vm1, R v0, R v1, R v2, R vlc) {
+__device__ __forceinline__ R omp6_limit_inl(R mid_nf, R vm2, R vm1, R v0, R v1, R v2, R vlc) {
   const R kappa = R(Omp6C::kappa);
   R d1 = vm2 + v0 - R(2) * vm1;
   R d2 = vm1 + v1 - R(2) * v0;
@@ -266,6 +277,10 @@ __device__ __noinline__ R omp6_limit(R mid_nf, R vm2, R vm1, R v0, R v1, R v2, R
   R fmin = rmax(rmin(rmin(v0, v1), md), rmin(rmin(v0, ul), lc));
   R fmax = rmin(rmax(rmax(v0, v1), md), rmax(rmax(v0, ul), lc));
   return mid_nf + minmod2(fmax - mid_nf, fmin - mid_nf);
+}
+template <typename R>
+__device__ __noinline__ R omp6_limit(R mid_nf, R vm2, R vm1, R v0, R v1, R v2, R vlc) {
+  return omp6_limit_inl(mid_nf, vm2, vm1, v0, v1, v2, vlc);
 }
 
 // hh_OMP6P: OCFD_Schemes_1.f90:195-226 (OCFD_OMP6P, OCFD_Schemes.f90:201-234)

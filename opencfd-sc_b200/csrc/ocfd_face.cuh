@@ -26,9 +26,13 @@
 
 namespace ocfd {
 
-// Tile shapes (NP pencils x TF faces, NP*TF = 256).  Variant 0 is the
-// default of the single-instance launches; variant 1 (TF = 32) wastes fewer
-// threads on short pencils and is one of the choices of the batch autotuner.
+// Tile shapes (NP pencils x TF faces, one face per thread).  Variants 0 and 1
+// (256 threads) are the choices of the batch autotuner -- variant 1 (TF = 32)
+// wastes fewer threads on short pencils.  Variant 2 (128 threads) is the
+// single-instance default: at 256^3 it measured 5-9% faster than variant 0 on
+// the FP64 characteristic sweeps (four blocks per SM overlap one another's
+// barrier and load phases better than two) and equal elsewhere.  Variants 3
+// (64 threads) and 4 (128 threads, TF = 32 along y and z) measured slower.
 template <int DIR, int V>
 struct FaceTileV;
 template <>
@@ -55,11 +59,44 @@ template <>
 struct FaceTileV<2, 1> {
   static constexpr int NP = 8, TF = 32;
 };
+// 128-thread tiles (more, smaller blocks per SM)
+template <>
+struct FaceTileV<0, 2> {
+  static constexpr int NP = 2, TF = 64;
+};
+template <>
+struct FaceTileV<1, 2> {
+  static constexpr int NP = 8, TF = 16;
+};
+template <>
+struct FaceTileV<2, 2> {
+  static constexpr int NP = 8, TF = 16;
+};
+template <>
+struct FaceTileV<0, 3> {
+  static constexpr int NP = 1, TF = 64;
+};
+template <>
+struct FaceTileV<1, 3> {
+  static constexpr int NP = 4, TF = 16;
+};
+template <>
+struct FaceTileV<2, 3> {
+  static constexpr int NP = 4, TF = 16;
+};
+template <>
+struct FaceTileV<1, 4> {
+  static constexpr int NP = 4, TF = 32;
+};
+template <>
+struct FaceTileV<2, 4> {
+  static constexpr int NP = 4, TF = 32;
+};
 #ifndef OCFD_FACE_X_VARIANT
-#define OCFD_FACE_X_VARIANT 0
+#define OCFD_FACE_X_VARIANT 2
 #endif
 #ifndef OCFD_FACE_YZ_VARIANT
-#define OCFD_FACE_YZ_VARIANT 0
+#define OCFD_FACE_YZ_VARIANT 2
 #endif
 template <int DIR>
 struct FaceTile : FaceTileV<DIR, DIR == 0 ? OCFD_FACE_X_VARIANT : OCFD_FACE_YZ_VARIANT> {};
@@ -222,8 +259,9 @@ struct Stencil<SCH_WENO5> {
 // side) -- and the whole block evaluates the queue, one entry per thread:
 // eigenvector row, the five projected stencil values and the limiter.  The
 // capacity is ten entries per face, so the queue never overflows.
+template <int NF>  // faces (threads) per block
 struct LimQueue {
-  static constexpr int CAP = 2560;
+  static constexpr int CAP = 10 * NF;
   template <typename R>
   static constexpr size_t bytes() {
     return ((size_t)CAP * sizeof(R) + (CAP + 1) * sizeof(int) + 15) / 16 * 16;
@@ -374,8 +412,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   // the 17 staged arrays -- CAP unlimited values, CAP tags (window offset * 16 +
   // component * 2 + side), the entry count
   constexpr bool DEFER = CHAR && SCHEME == SCH_OMP6 && OCFD_FEWER_DIVS;
-  constexpr int JC = LimQueue::CAP;
-  static_assert(!DEFER || NP * TF == 256, "the deferred limiter assumes one face per thread");
+  constexpr int JC = LimQueue<NP * TF>::CAP;  // one face per thread: blockDim.x == NP * TF
   R* const jv = sm + 17 * NP * LT;
   int* const jtag = reinterpret_cast<int*>(jv + JC);
   int* const jn = jtag + JC;
@@ -870,8 +907,11 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #define OCFD_FACE32_MINB 4
 #endif
 #define OCFD_FACE_MINB (sizeof(R) == 8 ? 2 : OCFD_FACE32_MINB)
+// threads and minimum resident blocks of the single-instance sweeps (tile FaceTile<DIR>)
+#define OCFD_FACE_NT(DIR) (FaceTile<DIR>::NP * FaceTile<DIR>::TF)
+#define OCFD_FACE_BOUNDS(DIR) __launch_bounds__(OCFD_FACE_NT(DIR), OCFD_FACE_MINB * 256 / OCFD_FACE_NT(DIR))
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
-__global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face(FaceArgs<S> a) {
+__global__ void OCFD_FACE_BOUNDS(DIR) k_face(FaceArgs<S> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR>::NP, FaceTile<DIR>::TF, R, S>(
       a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
@@ -893,7 +933,7 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<Fac
 // Single-instance sweep of a periodic direction with the input tiles staged by
 // TMA (the arithmetic is that of k_face).
 template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
-__global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
+__global__ void OCFD_FACE_BOUNDS(DIR) k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
   constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -945,7 +985,7 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_tma(FaceArgs<S> a,
 template <int DIR, bool CHAR, int NP, int TF, typename R>
 constexpr size_t face_smem() {
   // split fluxes (+ face state and the limiter queue)
-  return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R) + (CHAR ? LimQueue::bytes<R>() : 0);
+  return (size_t)(CHAR ? 17 : 10) * NP * (TF + 7) * sizeof(R) + (CHAR ? LimQueue<NP * TF>::template bytes<R>() : 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -29,10 +29,11 @@ namespace ocfd {
 // Tile shapes (NP pencils x TF faces, one face per thread).  Variants 0 and 1
 // (256 threads) are the choices of the batch autotuner -- variant 1 (TF = 32)
 // wastes fewer threads on short pencils.  Variant 2 (128 threads) is the
-// single-instance default: at 256^3 it measured 5-9% faster than variant 0 on
-// the FP64 characteristic sweeps (four blocks per SM overlap one another's
-// barrier and load phases better than two) and equal elsewhere.  Variants 3
-// (64 threads) and 4 (128 threads, TF = 32 along y and z) measured slower.
+// single-instance tile of the characteristic OMP6 sweeps: at 256^3 it measured
+// 5-9% faster there than variant 0 (four blocks per SM overlap one another's
+// barrier and load phases better than two), but slower on the hybrid and
+// WENO7 sweeps, which keep variant 0.  Variants 3 (64 threads) and 4 (128
+// threads, TF = 32 along y and z) measured slower.
 template <int DIR, int V>
 struct FaceTileV;
 template <>
@@ -92,14 +93,9 @@ template <>
 struct FaceTileV<2, 4> {
   static constexpr int NP = 4, TF = 32;
 };
-#ifndef OCFD_FACE_X_VARIANT
-#define OCFD_FACE_X_VARIANT 2
-#endif
-#ifndef OCFD_FACE_YZ_VARIANT
-#define OCFD_FACE_YZ_VARIANT 2
-#endif
-template <int DIR>
-struct FaceTile : FaceTileV<DIR, DIR == 0 ? OCFD_FACE_X_VARIANT : OCFD_FACE_YZ_VARIANT> {};
+// tile of a single-instance sweep
+template <int DIR, bool CHAR, int SCHEME>
+struct FaceTile : FaceTileV<DIR, (CHAR && SCHEME == SCH_OMP6) ? 2 : 0> {};
 
 // Grid of one launch: (x, y, z) blocks for a face sweep of instance a.
 template <int DIR, int NP, int TF, typename S>
@@ -907,13 +903,13 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #define OCFD_FACE32_MINB 4
 #endif
 #define OCFD_FACE_MINB (sizeof(R) == 8 ? 2 : OCFD_FACE32_MINB)
-// threads and minimum resident blocks of the single-instance sweeps (tile FaceTile<DIR>)
-#define OCFD_FACE_NT(DIR) (FaceTile<DIR>::NP * FaceTile<DIR>::TF)
-#define OCFD_FACE_BOUNDS(DIR) __launch_bounds__(OCFD_FACE_NT(DIR), OCFD_FACE_MINB * 256 / OCFD_FACE_NT(DIR))
+// threads and minimum resident blocks of the single-instance sweeps
+#define OCFD_FACE_NT (FaceTile<DIR, CHAR, SCHEME>::NP * FaceTile<DIR, CHAR, SCHEME>::TF)
+#define OCFD_FACE_BOUNDS __launch_bounds__(OCFD_FACE_NT, OCFD_FACE_MINB * 256 / OCFD_FACE_NT)
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
-__global__ void OCFD_FACE_BOUNDS(DIR) k_face(FaceArgs<S> a) {
+__global__ void OCFD_FACE_BOUNDS k_face(FaceArgs<S> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR>::NP, FaceTile<DIR>::TF, R, S>(
+  face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR, CHAR, SCHEME>::NP, FaceTile<DIR, CHAR, SCHEME>::TF, R, S>(
       a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
 }
 
@@ -933,8 +929,8 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<Fac
 // Single-instance sweep of a periodic direction with the input tiles staged by
 // TMA (the arithmetic is that of k_face).
 template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
-__global__ void OCFD_FACE_BOUNDS(DIR) k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
-  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+__global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
+  constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
@@ -991,7 +987,7 @@ constexpr size_t face_smem() {
 // ---------------------------------------------------------------------------
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
 static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
-  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+  constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   constexpr size_t smem = face_smem<DIR, CHAR, NP, TF, R>();
   auto kern = k_face<DIR, CHAR, SCHEME, ALLIN, R, S>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1054,7 +1050,7 @@ inline bool tma_strides_ok(const Grid& g) {
 
 template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
 static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
-  constexpr int NP = FaceTile<DIR>::NP, TF = FaceTile<DIR>::TF;
+  constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
   constexpr size_t smem = 128 + 8 * (size_t)B::SLOT + face_smem<DIR, CHAR, NP, TF, R>();
   auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S>;

@@ -424,7 +424,7 @@ def run_ours(args):
                          "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
                          "note": ("the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM "
                                   "bound: ncu pipe and DRAM fractions per kernel in "
-                                  "profiles/kernels_tgv128_omp6_char.md")},
+                                  "profiles/kernels_tgv192_omp6_char.md")},
             "cpu_baseline": cpu,
             "kinetic_energy": ke,
         }

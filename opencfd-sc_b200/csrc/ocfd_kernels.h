@@ -27,7 +27,7 @@ struct ViscArgs {
   const S* w;
   const S* T;
   const S* met[22];  // haloed metrics (OCFD_M_* order); S = double or float copies
-  R* ev;             // 12 interior arrays: Ev1(1..4), Ev2(1..4), Ev3(1..4)
+  R* ev;             // Ev1..Ev3, interior points, (d*n + point)*4 + component
 };
 
 // Arguments of the stage-tail kernels (flux difference, viscous divergence,
@@ -41,7 +41,7 @@ struct UpdArgs {
   long long fs[3];     // per-variable strides
   int fper[3];         // faces stored 1..n (periodic: face 0 == face n)
   double h_1[3];       // 1/hx, 1/hy, 1/hz
-  const R* ev;         // viscous fluxes (12 interior arrays) or nullptr
+  const R* ev;         // viscous fluxes ((d*n + point)*4 + component) or nullptr
   const double* ajac;  // haloed Ajac
   const double* pd;    // haloed d,u,v,w (mass force)
   const double* pu;

@@ -9,6 +9,7 @@
 // The stage-by-stage C ABI uses the unfused kernels below; both share the same
 // device functions, so they produce the same bits.
 #include <algorithm>
+#include <utility>
 
 #include "ocfd_kernels.h"
 #include "ocfd_schemes.cuh"
@@ -16,8 +17,9 @@
 // Minimum resident blocks per SM requested for the viscous-gradient and
 // stage-tail kernels (both memory-latency bound: more resident warps keep
 // more loads in flight, at the price of registers).  Measured best on B200 at
-// 256^3: FP64 tail 5, FP32 tail 6, FP64 viscous 4, FP32 viscous 6 (against
-// 2-3 blocks with the compiler's own register choice).
+// 256^3: FP64 tail 4, FP32 tail 5 (with the interleaved viscous fluxes; 5 and
+// 6 before), FP64 viscous 4, FP32 viscous 6 (against 2-3 blocks with the
+// compiler's own register choice).
 #ifndef OCFD_VISC64_MINB
 #define OCFD_VISC64_MINB 4
 #endif
@@ -25,10 +27,10 @@
 #define OCFD_VISC32_MINB 6
 #endif
 #ifndef OCFD_TAIL64_MINB
-#define OCFD_TAIL64_MINB 5
+#define OCFD_TAIL64_MINB 4
 #endif
 #ifndef OCFD_TAIL32_MINB
-#define OCFD_TAIL32_MINB 6
+#define OCFD_TAIL32_MINB 5
 #endif
 #define OCFD_VISC_MINB (sizeof(R) == 8 ? OCFD_VISC64_MINB : OCFD_VISC32_MINB)
 #define OCFD_TAIL_MINB (sizeof(R) == 8 ? OCFD_TAIL64_MINB : OCFD_TAIL32_MINB)
@@ -51,11 +53,52 @@ __device__ __forceinline__ D0C<R> d0c(const DCoef& c, int dir) {
                 R(c.c1[dir]), R(c.c2[dir]), R(c.c3[dir]), R(c.c4[dir])};
 }
 
+// Four values operated on element by element (the four viscous-flux components
+// of one direction, differentiated together); each element sees exactly the
+// scalar operations.
+template <typename R>
+struct V4 {
+  R v[4];
+};
+template <typename R>
+__device__ __forceinline__ V4<R> operator+(const V4<R>& a, const V4<R>& b) {
+  return V4<R>{{a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2], a.v[3] + b.v[3]}};
+}
+template <typename R>
+__device__ __forceinline__ V4<R> operator-(const V4<R>& a, const V4<R>& b) {
+  return V4<R>{{a.v[0] - b.v[0], a.v[1] - b.v[1], a.v[2] - b.v[2], a.v[3] - b.v[3]}};
+}
+template <typename R>
+__device__ __forceinline__ V4<R> operator*(R c, const V4<R>& a) {
+  return V4<R>{{c * a.v[0], c * a.v[1], c * a.v[2], c * a.v[3]}};
+}
+template <typename R>
+__device__ __forceinline__ V4<R> operator/(const V4<R>& a, R c) {
+  return V4<R>{{a.v[0] / c, a.v[1] / c, a.v[2] / c, a.v[3] / c}};
+}
+// the four components of one point of an interleaved viscous-flux array
+__device__ __forceinline__ V4<double> ldg4(const double* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return V4<double>{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ V4<float> ldg4(const float* p) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+  return V4<float>{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ void st4(double* p, double a, double b, double c, double d) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+  reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+}
+__device__ __forceinline__ void st4(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+
 // Closures only: called for l in {1,2,3,(4)} or {(n-3),n-2,n-1,n}, never reads
-// outside 1..n along the direction (the Ev arrays carry no halo).
-template <typename R, typename F>
-__device__ __forceinline__ R d0_bnd(F at, int l, int nn, int cd8, D0C<R> k) {
-  R r = R(0);
+// outside 1..n along the direction (the Ev arrays carry no halo).  V: the
+// accessor's value type (R, or V4<R> for four components at once).
+template <typename R, typename F, typename V = decltype(std::declval<F>()(0))>
+__device__ __forceinline__ V d0_bnd(F at, int l, int nn, int cd8, D0C<R> k) {
+  V r = V();
   if (l == 1) r = (R(-3) * at(0) + R(4) * at(1) - at(2)) / (R(2) * k.h);
   else if (l == 2) r = (at(1) - at(-1)) / (R(2) * k.h);
   else if (l == 3) r = (R(8) * (at(1) - at(-1)) - (at(2) - at(-2))) / (R(12) * k.h);
@@ -67,14 +110,14 @@ __device__ __forceinline__ R d0_bnd(F at, int l, int nn, int cd8, D0C<R> k) {
   return r;
 }
 
-template <typename R, typename F>
-__device__ __forceinline__ R d0(F at, int l, int nn, int periodic, int cd8, D0C<R> k) {
+template <typename R, typename F, typename V = decltype(std::declval<F>()(0))>
+__device__ __forceinline__ V d0(F at, int l, int nn, int periodic, int cd8, D0C<R> k) {
   const int lo = cd8 ? 4 : 3, hi = cd8 ? nn - 3 : nn - 2;
   if (periodic || (l > lo && l < hi)) {
     if (!cd8) return k.a1 * (at(3) - at(-3)) + k.a2 * (at(2) - at(-2)) + k.a3 * (at(1) - at(-1));
     return k.c1 * (at(1) - at(-1)) + k.c2 * (at(2) - at(-2)) + k.c3 * (at(3) - at(-3)) + k.c4 * (at(4) - at(-4));
   }
-  return d0_bnd<R>(at, l, nn, cd8, k);
+  return d0_bnd<R, F, V>(at, l, nn, cd8, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -137,13 +180,13 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
   const R E3 = uu * s13 + vv * s23 + ww * s33 + Amuk * Tz;
   const long long o = G.ii(i, j, k);
   const long long n = G.n;
+  // Ev stored direction by direction, the four components of a point together:
+  // element (d, point o, component m) at (d*n + o)*4 + m
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const R A1 = M[13 + 3 * d], A2 = M[14 + 3 * d], A3 = M[15 + 3 * d];
-    a.ev[o + (4 * d + 0) * n] = A1 * s11 + A2 * s12 + A3 * s13;
-    a.ev[o + (4 * d + 1) * n] = A1 * s12 + A2 * s22 + A3 * s23;
-    a.ev[o + (4 * d + 2) * n] = A1 * s13 + A2 * s23 + A3 * s33;
-    a.ev[o + (4 * d + 3) * n] = A1 * E1 + A2 * E2 + A3 * E3;
+    st4(a.ev + ((long long)d * n + o) * 4, A1 * s11 + A2 * s12 + A3 * s13, A1 * s12 + A2 * s22 + A3 * s23,
+        A1 * s13 + A2 * s23 + A3 * s33, A1 * E1 + A2 * E2 + A3 * E3);
   }
 }
 
@@ -281,29 +324,27 @@ __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int 
   bool wz[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) wz[d] = a.ph.periodic[d] && (lc[d] <= 4 || lc[d] > G.len(d) - 4);
+  V4<R> s[3];
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    R s[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const R* E = a.ev + (4 * d + m) * n + o;
-      const int l = lc[d], nn = G.len(d);
-      const int per = a.ph.periodic[d];
-      const long long st = is[d];
-      if (!wz[d]) {
-        auto at = [&](int off) -> R { return __ldg(E + (long long)off * st); };
-        s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
-      } else {
-        auto at = [&](int off) -> R {
-          int l2 = l + off;
-          l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
-          return __ldg(E + (long long)(l2 - l) * st);
-        };
-        s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
-      }
+  for (int d = 0; d < 3; d++) {
+    const R* E = a.ev + ((long long)d * n + o) * 4;
+    const int l = lc[d], nn = G.len(d);
+    const int per = a.ph.periodic[d];
+    const long long st = is[d] * 4;
+    if (!wz[d]) {
+      auto at = [&](int off) -> V4<R> { return ldg4(E + (long long)off * st); };
+      s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
+    } else {
+      auto at = [&](int off) -> V4<R> {
+        int l2 = l + off;
+        l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
+        return ldg4(E + (long long)(l2 - l) * st);
+      };
+      s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
     }
-    du[m + 1] = du[m + 1] + (s[0] + s[1] + s[2]) * ajac;
   }
+#pragma unroll
+  for (int m = 0; m < 4; m++) du[m + 1] = du[m + 1] + (s[0].v[m] + s[1].v[m] + s[2].v[m]) * ajac;
 }
 
 // primitive recovery of one point (comput_duvwT, OCFD_Time_Adv.f90:48-52)

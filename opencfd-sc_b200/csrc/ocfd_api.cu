@@ -697,6 +697,10 @@ static UpdArgs<R> upd_args(ocfd_handle* h) {
   a.st = h->dstat;
   a.krk = 1;
   a.fuse_bc = h->fuse_bc ? 1 : 0;
+  // between the stages of a step only the FP32 copies of d,u,v,w are read (the
+  // hybrid sensor runs at stage 1 on the previous step's FP64 values; the mass
+  // force reads the FP64 values, so it keeps them)
+  a.lean = (h->mixed && h->fuse_bc && h->p.if_mass_force != 1) ? 1 : 0;
   a.visc = h->p.if_viscous ? 1 : 0;
   a.chr = h->chr ? 1 : 0;
   return a;

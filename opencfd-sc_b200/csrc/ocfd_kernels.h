@@ -56,6 +56,8 @@ struct UpdArgs {
   DevStatus* st;
   int krk;
   int fuse_bc;         // BC_None without ghost cells: face refresh + halo in-kernel
+  int lean;            // mixed + fuse_bc: stages 1-2 leave the FP64 d,u,v,w unwritten
+                       // (nothing reads them before stage 3 rewrites them)
   int visc;
   int chr;
 };

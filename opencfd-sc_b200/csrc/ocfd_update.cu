@@ -484,10 +484,13 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
   if (FUSEBC && on_boundary_face(G, i, j, k)) refresh_of(q, a.ph.cv, fv);
 #pragma unroll
   for (int m = 0; m < 5; m++) a.f[o + m * n] = fv[m];
+  const int m0 = (a.lean && a.krk < 3) ? 4 : 0;  // lean stages: FP64 T only
 #pragma unroll
   for (int m = 0; m < 5; m++) {
-    a.prim[m][h] = q[m];
-    if (FUSEBC) mirror(G, a.ph.periodic, a.prim[m], i, j, k, q[m]);
+    if (m >= m0) {
+      a.prim[m][h] = q[m];
+      if (FUSEBC) mirror(G, a.ph.periodic, a.prim[m], i, j, k, q[m]);
+    }
     if (a.p32[0]) {
       a.p32[m][h] = float(q[m]);
       if (FUSEBC) mirror32(G, a.ph.periodic, a.p32[m], i, j, k, float(q[m]));
@@ -666,9 +669,16 @@ __device__ __forceinline__ void negt_fix_body(const UpdArgs<double>& a) {
       mirror(G, a.ph.periodic, Tn, i, j, k, T);
       if (a.p32[0]) mirror32(G, a.ph.periodic, a.p32[4], i, j, k, float(T));
       if (on_boundary_face(G, i, j, k)) {
-        double qv[5] = {a.prim[0][h], a.prim[1][h], a.prim[2][h], a.prim[3][h], T}, fv[5];
-        refresh_of(qv, a.ph.cv, fv);
         const long long o = G.ii(i, j, k);
+        double qv[5] = {a.prim[0][h], a.prim[1][h], a.prim[2][h], a.prim[3][h], T}, fv[5];
+        if (a.lean && a.krk < 3) {
+          // FP64 d,u,v,w were not written this stage: recover them from f
+          double fo[5], qo[5];
+          for (int m = 0; m < 5; m++) fo[m] = a.f[o + m * G.n];
+          prims_of(fo, a.ph.cv, a.ph.inv_cv, qo);
+          for (int m = 0; m < 4; m++) qv[m] = qo[m];
+        }
+        refresh_of(qv, a.ph.cv, fv);
         for (int m = 0; m < 5; m++) a.f[o + m * G.n] = fv[m];
       }
     }

@@ -32,7 +32,8 @@ struct ocfd_handle {
   double* du = nullptr;
   double* prim[5] = {};
   double* talt = nullptr;  // second temperature buffer (negative-T repair)
-  float* p32[5] = {};
+  float* p32[5] = {};  // mixed precision: FP32 copy of d in p32[0]; p32[1..4] stay null
+  float* q32 = nullptr;  // mixed precision: FP32 copies of u,v,w,T interleaved (4 floats a point)
   double* met[OCFD_N_METRICS] = {};
   float* met32[OCFD_N_METRICS] = {};
   double* rh = nullptr;
@@ -317,6 +318,7 @@ void ocfd_gpu_destroy(ocfd_handle* h) {
     F(h->prim[q]);
     F(h->p32[q]);
   }
+  F(h->q32);
   F(h->talt);
   for (int m = 0; m < OCFD_N_METRICS; m++) {
     F(h->met[m]);
@@ -382,7 +384,8 @@ int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
   for (int m = 0; m < OCFD_N_METRICS; m++) AL(h->met[m], nh * 8);
   AL(h->rh, nh * 8);
   if (h->mixed) {
-    for (int q = 0; q < 5; q++) AL(h->p32[q], nh * 4);
+    AL(h->p32[0], nh * 4);
+    AL(h->q32, nh * 16);
     for (int m = 0; m < OCFD_N_METRICS; m++) AL(h->met32[m], nh * 4);
   }
   for (int d = 0; d < 3; d++) {
@@ -411,7 +414,8 @@ int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
   k_fill<<<B, 256, 0, h->st>>>(h->f, 5 * n, 0.0);
   k_fill<<<B, 256, 0, h->st>>>(h->fn, 5 * n, 0.0);
   if (h->mixed) {
-    for (int q = 0; q < 5; q++) k_fill32<<<B, 256, 0, h->st>>>(h->p32[q], nh, 1.0f);
+    k_fill32<<<B, 256, 0, h->st>>>(h->p32[0], nh, 1.0f);
+    k_fill32<<<B, 256, 0, h->st>>>(h->q32, 4 * nh, 1.0f);
     for (int m = 0; m < OCFD_N_METRICS; m++) k_fill32<<<B, 256, 0, h->st>>>(h->met32[m], nh, 1.0f);
   }
   e = cudaMemsetAsync(h->dstat, 0, sizeof(DevStatus), h->st);
@@ -430,7 +434,8 @@ static int refresh_met32(ocfd_handle* h) {
 }
 static int refresh_p32(ocfd_handle* h) {
   if (!h->mixed) return OCFD_OK;
-  for (int q = 0; q < 5; q++) CK(launch_to_f32(h->prim[q], h->p32[q], h->g.nh, h->st));
+  CK(launch_to_f32(h->prim[0], h->p32[0], h->g.nh, h->st));
+  CK(launch_to_f32x4(h->prim[1], h->prim[2], h->prim[3], h->prim[4], h->q32, h->g.nh, h->st));
   return OCFD_OK;
 }
 
@@ -590,9 +595,13 @@ static int halo_all(ocfd_handle* h) {
   CK(launch_halo(h->g, h->ph.periodic, L, h->st));
   if (h->mixed) {
     PtrList<float> L32;
-    L32.n = 5;
-    for (int q = 0; q < 5; q++) L32.p[q] = h->p32[q];
+    L32.n = 1;
+    L32.p[0] = h->p32[0];
     CK(launch_halo_f32(h->g, h->ph.periodic, L32, h->st));
+    PtrList<float4> L4;
+    L4.n = 1;
+    L4.p[0] = reinterpret_cast<float4*>(h->q32);
+    CK(launch_halo_f32x4(h->g, h->ph.periodic, L4, h->st));
   }
   return OCFD_OK;
 }
@@ -628,12 +637,11 @@ static FaceArgs<S> face_args(ocfd_handle* h, int d) {
   FaceArgs<S> a;
   a.g = g;
   a.ph = h->ph;
+  a.q4 = nullptr;
   if (std::is_same<S, float>::value) {
     a.d = (const S*)h->p32[0];
-    a.u = (const S*)h->p32[1];
-    a.v = (const S*)h->p32[2];
-    a.w = (const S*)h->p32[3];
-    a.T = (const S*)h->p32[4];
+    a.u = a.v = a.w = a.T = nullptr;
+    a.q4 = h->q32;
     a.A1 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d];
     a.A2 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 1];
     a.A3 = (const S*)h->met32[OCFD_M_AKX1 + 3 * d + 2];
@@ -694,6 +702,7 @@ static UpdArgs<R> upd_args(ocfd_handle* h) {
   a.prim[4] = h->talt;  // written; becomes current after the swap
   a.told = h->prim[4];
   for (int q = 0; q < 5; q++) a.p32[q] = h->mixed ? h->p32[q] : nullptr;
+  a.q32 = h->mixed ? h->q32 : nullptr;
   a.st = h->dstat;
   a.krk = 1;
   a.fuse_bc = h->fuse_bc ? 1 : 0;
@@ -738,12 +747,11 @@ static ViscArgs<R, S> visc_args(ocfd_handle* h) {
   a.g = h->g;
   a.ph = h->ph;
   a.dc = h->dc;
+  a.q4 = nullptr;
   if (std::is_same<S, float>::value) {
     a.d = (const S*)h->p32[0];
-    a.u = (const S*)h->p32[1];
-    a.v = (const S*)h->p32[2];
-    a.w = (const S*)h->p32[3];
-    a.T = (const S*)h->p32[4];
+    a.u = a.v = a.w = a.T = nullptr;
+    a.q4 = h->q32;
     for (int m = 0; m < 22; m++) a.met[m] = (const S*)h->met32[m];
   } else {
     a.d = (const S*)h->prim[0];

@@ -187,6 +187,7 @@ struct FaceArgs {
   const S* v;
   const S* w;
   const S* T;
+  const float* q4;   // FP32 sweeps: u,v,w,T interleaved (haloed, 4 floats a point); u..T unused
   const S* A1;
   const S* A2;
   const S* A3;

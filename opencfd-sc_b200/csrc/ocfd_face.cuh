@@ -444,10 +444,18 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
     } else if (ok) {
       long long h = G.ih(i, j, k) + (long long)gl * hs;
       d = R(__ldg(a.d + h));
-      u = R(__ldg(a.u + h));
-      v = R(__ldg(a.v + h));
-      w = R(__ldg(a.w + h));
-      T = R(__ldg(a.T + h));
+      if constexpr (sizeof(S) == 4) {  // FP32 copies: u,v,w,T interleaved
+        const float4 t = __ldg(reinterpret_cast<const float4*>(a.q4) + h);
+        u = R(t.x);
+        v = R(t.y);
+        w = R(t.z);
+        T = R(t.w);
+      } else {
+        u = R(__ldg(a.u + h));
+        v = R(__ldg(a.v + h));
+        w = R(__ldg(a.w + h));
+        T = R(__ldg(a.T + h));
+      }
       A1 = met_at<R>(ph, 13 + 3 * DIR, a.A1, h);
       A2 = met_at<R>(ph, 14 + 3 * DIR, a.A2, h);
       A3 = met_at<R>(ph, 15 + 3 * DIR, a.A3, h);

@@ -26,6 +26,7 @@ struct ViscArgs {
   const S* v;
   const S* w;
   const S* T;
+  const float* q4;   // FP32 instances: u,v,w,T interleaved (haloed, 4 floats a point); u..T unused
   const S* met[22];  // haloed metrics (OCFD_M_* order); S = double or float copies
   R* ev;             // Ev1..Ev3, interior points, (d*n + point)*4 + component
 };
@@ -52,7 +53,8 @@ struct UpdArgs {
   const double* fn;
   double* prim[5];     // haloed d,u,v,w,T (T: the buffer being written)
   const double* told;  // haloed T of the previous stage (negative-T repair)
-  float* p32[5];       // FP32 copies of the primitives (mixed precision) or nullptr
+  float* p32[5];       // FP32 copy of d in p32[0] (mixed precision) or nullptr; p32[1..4] unused
+  float* q32;          // FP32 copies of u,v,w,T interleaved, 4 floats a haloed point
   DevStatus* st;
   int krk;
   int fuse_bc;         // BC_None without ghost cells: face refresh + halo in-kernel
@@ -156,6 +158,7 @@ inline dim3 update_dims(const Grid& g) { return dim3((g.nx + 31) / 32, (g.ny + 7
 
 // periodic face halo of narr haloed arrays (exchange_boundary_xyz)
 cudaError_t launch_halo(const Grid& g, const int periodic[3], PtrList<double> arrs, cudaStream_t st);
+cudaError_t launch_halo_f32x4(const Grid& g, const int periodic[3], PtrList<float4> arrs, cudaStream_t st);
 cudaError_t launch_halo_f32(const Grid& g, const int periodic[3], PtrList<float> arrs, cudaStream_t st);
 // BC dispatch on the primitives (blunt2d / user isothermal wall)
 cudaError_t launch_bc_wall(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
@@ -183,6 +186,8 @@ cudaError_t launch_bc_refresh(const Grid& g, const Phys& ph, double* f, double* 
 // Flow_Ghost_Extent_2nd
 cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
 // FP32 copies of the primitives
+cudaError_t launch_to_f32x4(const double* u, const double* v, const double* w, const double* T, float* dst, long long n,
+                            cudaStream_t st);
 cudaError_t launch_to_f32(const double* src, float* dst, long long n, cudaStream_t st);
 // init3d: f from primitives
 cudaError_t launch_init3d(const Grid& g, const Phys& ph, double* f, double* const prim[5], cudaStream_t st);

@@ -86,6 +86,7 @@ __device__ __forceinline__ V4<float> ldg4(const float* p) {
   return V4<float>{{a.x, a.y, a.z, a.w}};
 }
 __device__ __forceinline__ void st4(double* p, double a, double b, double c, double d) {
+  // two 16-byte stores (four scalar stores measured 10% slower in the viscous kernel)
   reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
   reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
 }
@@ -133,17 +134,39 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
   const long long c = G.ih(i, j, k);
   const int cd8 = a.ph.scheme_vis == 6;
   const int lcoord[3] = {i, j, k};
-  const S* q4[4] = {a.u, a.v, a.w, a.T};
   R gr[4][3];  // [u,v,w,T][k,i,s]
-#pragma unroll
-  for (int q = 0; q < 4; q++)
+  R uu, vv, ww, T;
+  if constexpr (sizeof(S) == 4) {
+    // FP32 copies: u,v,w,T interleaved, one 16-byte load per stencil point
+    const float4* base = reinterpret_cast<const float4*>(a.q4) + c;
 #pragma unroll
     for (int dir = 0; dir < 3; dir++) {
       const long long hs = G.hstride(dir);
-      const S* base = q4[q] + c;
-      auto at = [&](int off) -> R { return R(__ldg(base + off * hs)); };
-      gr[q][dir] = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, d0c<R>(a.dc, dir));
+      auto at = [&](int off) -> V4<R> {
+        const float4 t = __ldg(base + off * hs);
+        return V4<R>{{R(t.x), R(t.y), R(t.z), R(t.w)}};
+      };
+      const V4<R> g4 = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, d0c<R>(a.dc, dir));
+#pragma unroll
+      for (int q = 0; q < 4; q++) gr[q][dir] = g4.v[q];
     }
+    const float4 t = __ldg(base);
+    uu = R(t.x);
+    vv = R(t.y);
+    ww = R(t.z);
+    T = R(t.w);
+  } else {
+    const S* q4[4] = {a.u, a.v, a.w, a.T};
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int dir = 0; dir < 3; dir++) {
+        const long long hs = G.hstride(dir);
+        const S* base = q4[q] + c;
+        auto at = [&](int off) -> R { return R(__ldg(base + off * hs)); };
+        gr[q][dir] = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, d0c<R>(a.dc, dir));
+      }
+  }
   R M[22];
 #pragma unroll
   for (int m = 3; m < 22; m++) M[m] = met_at<R>(a.ph, m, a.met[m], c);
@@ -164,7 +187,7 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
   const R div = ux + vy + wz;
   // Sutherland viscosity, comput_Amu
   const R Tsb = R(110.4 / a.ph.ref_amu_t0), TmpR = R(1.0 / a.ph.re);
-  const R T = R(__ldg(a.T + c));
+  if constexpr (sizeof(S) != 4) T = R(__ldg(a.T + c));
   const R Amu = TmpR * (R(1) + Tsb) * sqrt(T * T * T) / (Tsb + T);
   const R Amuk = R(a.ph.cp) * Amu / R(a.ph.pr);
   const R t23 = R(2.0 / 3.0);
@@ -174,7 +197,11 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
   const R s12 = (uy + vx) * Amu;
   const R s13 = (uz + wx) * Amu;
   const R s23 = (vz + wy) * Amu;
-  const R uu = R(__ldg(a.u + c)), vv = R(__ldg(a.v + c)), ww = R(__ldg(a.w + c));
+  if constexpr (sizeof(S) != 4) {
+    uu = R(__ldg(a.u + c));
+    vv = R(__ldg(a.v + c));
+    ww = R(__ldg(a.w + c));
+  }
   const R E1 = uu * s11 + vv * s12 + ww * s13 + Amuk * Tx;
   const R E2 = uu * s12 + vv * s22 + ww * s23 + Amuk * Ty;
   const R E3 = uu * s13 + vv * s23 + ww * s33 + Amuk * Tz;
@@ -410,6 +437,37 @@ __device__ __forceinline__ void mirror32(const Grid& G, const int* per, float* p
   }
 }
 
+// the same for one component (stride 4, offset c) of an interleaved FP32 array
+__device__ __forceinline__ void mirror32c(const Grid& G, const int* per, float* p, int c, int i, int j, int k,
+                                          float x) {
+  if (per[0]) {
+    if (i <= LAP) p[4 * G.ih(i + G.nx, j, k) + c] = x;
+    if (i > G.nx - LAP) p[4 * G.ih(i - G.nx, j, k) + c] = x;
+  }
+  if (per[1]) {
+    if (j <= LAP) p[4 * G.ih(i, j + G.ny, k) + c] = x;
+    if (j > G.ny - LAP) p[4 * G.ih(i, j - G.ny, k) + c] = x;
+  }
+  if (per[2]) {
+    if (k <= LAP) p[4 * G.ih(i, j, k + G.nz) + c] = x;
+    if (k > G.nz - LAP) p[4 * G.ih(i, j, k - G.nz) + c] = x;
+  }
+}
+__device__ __forceinline__ void mirror4(const Grid& G, const int* per, float4* p, int i, int j, int k, float4 x) {
+  if (per[0]) {
+    if (i <= LAP) p[G.ih(i + G.nx, j, k)] = x;
+    if (i > G.nx - LAP) p[G.ih(i - G.nx, j, k)] = x;
+  }
+  if (per[1]) {
+    if (j <= LAP) p[G.ih(i, j + G.ny, k)] = x;
+    if (j > G.ny - LAP) p[G.ih(i, j - G.ny, k)] = x;
+  }
+  if (per[2]) {
+    if (k <= LAP) p[G.ih(i, j, k + G.nz)] = x;
+    if (k > G.nz - LAP) p[G.ih(i, j, k - G.nz)] = x;
+  }
+}
+
 __device__ __forceinline__ void record_negt(DevStatus* st, long long h) {
   int slot = atomicAdd(&st->negt_count, 1);
   if (slot < 16) st->negt_list[slot] = (int)h;
@@ -491,10 +549,14 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
       a.prim[m][h] = q[m];
       if (FUSEBC) mirror(G, a.ph.periodic, a.prim[m], i, j, k, q[m]);
     }
-    if (a.p32[0]) {
-      a.p32[m][h] = float(q[m]);
-      if (FUSEBC) mirror32(G, a.ph.periodic, a.p32[m], i, j, k, float(q[m]));
-    }
+  }
+  if (a.p32[0]) {
+    a.p32[0][h] = float(q[0]);
+    if (FUSEBC) mirror32(G, a.ph.periodic, a.p32[0], i, j, k, float(q[0]));
+    const float4 x = make_float4(float(q[1]), float(q[2]), float(q[3]), float(q[4]));
+    float4* q4 = reinterpret_cast<float4*>(a.q32);
+    q4[h] = x;
+    if (FUSEBC) mirror4(G, a.ph.periodic, q4, i, j, k, x);
   }
 }
 
@@ -613,9 +675,10 @@ __global__ void __launch_bounds__(256) k_duvwt(UpdArgs<double> a) {
   const long long h = G.ih(i, j, k);
   if (q[4] <= 0.0) record_negt(a.st, h);
 #pragma unroll
-  for (int m = 0; m < 5; m++) {
-    a.prim[m][h] = q[m];
-    if (a.p32[0]) a.p32[m][h] = float(q[m]);
+  for (int m = 0; m < 5; m++) a.prim[m][h] = q[m];
+  if (a.p32[0]) {
+    a.p32[0][h] = float(q[0]);
+    reinterpret_cast<float4*>(a.q32)[h] = make_float4(float(q[1]), float(q[2]), float(q[3]), float(q[4]));
   }
 }
 cudaError_t launch_duvwt(const UpdArgs<double>& a, cudaStream_t st) {
@@ -664,10 +727,10 @@ __device__ __forceinline__ void negt_fix_body(const UpdArgs<double>& a) {
     const int i = (int)(h % G.nxh) - (LAP - 1);
     const int j = (int)((h / G.nxh) % G.nyh) - (LAP - 1);
     const int k = (int)(h / ((long long)G.nxh * G.nyh)) - (LAP - 1);
-    if (a.p32[0]) a.p32[4][h] = float(T);
+    if (a.p32[0]) a.q32[4 * h + 3] = float(T);
     if (a.fuse_bc) {
       mirror(G, a.ph.periodic, Tn, i, j, k, T);
-      if (a.p32[0]) mirror32(G, a.ph.periodic, a.p32[4], i, j, k, float(T));
+      if (a.p32[0]) mirror32c(G, a.ph.periodic, a.q32, 3, i, j, k, float(T));
       if (on_boundary_face(G, i, j, k)) {
         const long long o = G.ii(i, j, k);
         double qv[5] = {a.prim[0][h], a.prim[1][h], a.prim[2][h], a.prim[3][h], T}, fv[5];
@@ -766,6 +829,11 @@ __global__ void k_halo(Grid G, int px, int py, int pz, PtrList<T> arrs) {
 cudaError_t launch_halo(const Grid& g, const int periodic[3], PtrList<double> arrs, cudaStream_t st) {
   if (!periodic[0] && !periodic[1] && !periodic[2]) return cudaSuccess;
   k_halo<double><<<148 * 4, 256, 0, st>>>(g, periodic[0], periodic[1], periodic[2], arrs);
+  return cudaGetLastError();
+}
+cudaError_t launch_halo_f32x4(const Grid& g, const int periodic[3], PtrList<float4> arrs, cudaStream_t st) {
+  if (!periodic[0] && !periodic[1] && !periodic[2]) return cudaSuccess;
+  k_halo<float4><<<148 * 4, 256, 0, st>>>(g, periodic[0], periodic[1], periodic[2], arrs);
   return cudaGetLastError();
 }
 cudaError_t launch_halo_f32(const Grid& g, const int periodic[3], PtrList<float> arrs, cudaStream_t st) {
@@ -1079,6 +1147,16 @@ cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], c
   return cudaGetLastError();
 }
 
+__global__ void k_to_f32x4(const double* u, const double* v, const double* w, const double* T, float4* dst,
+                           long long n) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    dst[c] = make_float4(float(u[c]), float(v[c]), float(w[c]), float(T[c]));
+}
+cudaError_t launch_to_f32x4(const double* u, const double* v, const double* w, const double* T, float* dst, long long n,
+                            cudaStream_t st) {
+  k_to_f32x4<<<148 * 8, 256, 0, st>>>(u, v, w, T, reinterpret_cast<float4*>(dst), n);
+  return cudaGetLastError();
+}
 __global__ void k_to_f32(const double* src, float* dst, long long n) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
     dst[c] = float(src[c]);

@@ -121,8 +121,12 @@ def byte_model(p, zero_mask: int = 0) -> dict:
     nface = 5  # characteristic form: projected fluxes; flux-vector form: h(F+) + h(F-) per face
     face = {d: 5 * s + nz(range(13 + 3 * i, 16 + 3 * i)) * s + nface * r for i, d in enumerate(("x", "y", "z"))}
     visc = 4 * s + nz(range(3, 22)) * s + 12 * r  # u,v,w,T + non-zero metrics in; 12 Ev out
-    # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out
-    tail = 3 * nface * r + 12 * r + 8 + 40 + 40 * 2.0 / 3.0 + 40 + 40 + (20 if p.precision == 1 else 0)
+    # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out.
+    # Mixed precision on an all-periodic grid (BC_None, fused): stages 1-2 write only T of
+    # the FP64 primitives; FP32 copies of d and u,v,w,T (20 bytes) every stage.
+    lean = p.precision == 1 and all(p.iperiodic[d] for d in range(3)) and p.if_mass_force != 1
+    prims = (8 + 8 + 40) / 3.0 if lean else 40
+    tail = 3 * nface * r + 12 * r + 8 + 40 + 40 * 2.0 / 3.0 + 40 + prims + (20 if p.precision == 1 else 0)
     return {"face_x": face["x"], "face_y": face["y"], "face_z": face["z"], "visc_grad": visc, "stage_tail": tail}
 
 

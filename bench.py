@@ -362,8 +362,11 @@ def run_ours(args):
     bpp = load_traffic().get(f"{args.workload}:{args.precision}:{dom}")
     traffic = None if bpp is None else bpp * n  # DRAM bytes per launch, scaled from a 128^3 capture
 
-    # ---- end to end through the C ABI with host-owned state: per step, upload
-    # f + haloed primitives from pinned host memory, one time step, download them.
+    # ---- end to end through the C ABI with host-owned state.  Headline mode: the
+    # host owns the conserved variables f (the reference's time-loop state); per
+    # step f is uploaded from pinned host memory, the primitives are derived from
+    # it on the device (comput_duvwT), one time step runs and f is downloaded.
+    # Second mode: f and the haloed primitives both ways.
     K2 = max(1, min(args.steps, 5))
     f_host = torch.empty(s.shape5, dtype=torch.float64, pin_memory=True).numpy()
     prim_host = [torch.empty(s.shape_h, dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
@@ -377,17 +380,29 @@ def run_ours(args):
     istep, tt = s.time()
     if dist:
         tdist.barrier()
+    nneg = C.c_int(0)
+    t0 = time.perf_counter()
+    for _ in range(K2):
+        L.ocfd_gpu_upload_state(s.h, fptr, None, istep, tt)
+        L.ocfd_gpu_duvwt(s.h, C.byref(nneg))
+        L.ocfd_gpu_step(s.h, 1, 0)
+        L.ocfd_gpu_download_state(s.h, fptr, None)
+        istep, tt = s.time()
+    t_e2e = time.perf_counter() - t0
     t0 = time.perf_counter()
     for _ in range(K2):
         L.ocfd_gpu_upload_state(s.h, fptr, C.cast(parr, C.c_void_p), istep, tt)
         L.ocfd_gpu_step(s.h, 1, 0)
         L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
-    t_e2e = time.perf_counter() - t0
+        istep, tt = s.time()
+    t_full = time.perf_counter() - t0
     if dist:
-        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        t = torch.tensor([t_e2e, t_full], device=f"cuda:{local}", dtype=torch.float64)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+        t_e2e, t_full = float(t[0].item()), float(t[1].item())
     e2e = world * n * K2 / t_e2e / 1e9
+    e2e_full = world * n * K2 / t_full / 1e9
+    bytes_f = 5 * 8 * n
     bytes_state = 5 * 8 * (n + int(np.prod(s.shape_h)))
     s.sync()  # raises if the run hit the reference's negative-temperature stop
     ke = s.show_flow_msg()[1]
@@ -419,8 +434,12 @@ def run_ours(args):
                        "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (the state is GBs)"},
             "clocks": clocks,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state,
-                    "mode": "host-owned state: upload f + primitives, one step, download f + primitives"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_f, "d2h_bytes_per_step": bytes_f,
+                    "mode": "host-owned conserved state f: upload f, primitives derived on the device "
+                            "(comput_duvwT), one step, download f",
+                    "with_primitives": {"value": e2e_full, "h2d_bytes_per_step": bytes_state,
+                                        "d2h_bytes_per_step": bytes_state,
+                                        "mode": "upload f + haloed primitives, one step, download both"}},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

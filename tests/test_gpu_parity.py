@@ -244,6 +244,42 @@ def test_mixed_precision_close_to_fp64():
     assert abs(eb[1] - ea[1]) / ea[1] < 1e-6
 
 
+def test_mixed_step_leaves_consistent_fp64_primitives():
+    """Mixed precision on a periodic box: stages 1 and 2 of a step skip the FP64
+    d,u,v,w (only their FP32 copies are read before stage 3), so after every
+    step the FP64 primitives must again be those of f -- interior and periodic
+    halo images -- and a step continued from an uploaded f (primitives derived
+    on the device) must match the device-resident run."""
+    pm, _, prims = tgv_case(scheme=SCHEME_OMP6, character=1, mixed=True)
+    s = Solver(pm)
+    s.init_mesh()
+    s.init3d(prims)
+    g = pm.gamma
+    for _ in range(3):
+        s.step(1)
+        f, pr = s.download_state()
+        d = f[0]
+        u, v, w = f[1] / d, f[2] / d, f[3] / d
+        cv = 1.0 / (g * (g - 1.0) * pm.ma ** 2)
+        T = (f[4] - 0.5 * d * (u * u + v * v + w * w)) / (d * cv)
+        for q, ref in enumerate((d, u, v, w, T)):
+            assert rel_l2(interior(pr[q]), ref) < 1e-13
+        # periodic images: x halo planes equal the opposite interior planes
+        for q in range(5):
+            np.testing.assert_array_equal(pr[q][4:-4, 4:-4, 0:4], pr[q][4:-4, 4:-4, -8:-4])
+    f0 = s.download_f()
+    t = Solver(pm)
+    t.init_mesh()
+    t.init3d(prims)
+    t.upload_state(f=f0)
+    t.comput_duvwT()
+    s.step(2)
+    t.step(2)
+    assert rel_l2(t.download_f(), s.download_f()) < 1e-12
+    s.close()
+    t.close()
+
+
 def test_metric_zero_mask_box_and_curvilinear():
     """Box grids: exactly the twelve off-diagonal metric arrays are +0.0 where the
     kernels read them (their loads are skipped); on a body-fitted grid the

@@ -14,9 +14,12 @@
 //   time loop      (OCFD_NS_Solver.f90:21-78)  -> ocfd_gpu_step() in blocks of Istep_show,
 //                                                 show_flow_msg, save_flow_data at Istep_Save
 //   save_flow_data (OCFD_IO.f90:45-65)         -> OCFD%08d.dat writer
+//   OCFD_analysis  (OCFD_ANA.f90:3-31)         -> run_analysis(): the ANA_Para schedule
+//                                                 (codes 100-104) over the device analyses
 // Files use the reference's Fortran unformatted sequential records (4-byte
 // length markers): record 1 = (Istep:int32, tt:real64), then for each of
 // d,u,v,w,T nz records of nx*ny real64 (OCFD_IO_mpi.f90:132-282).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -158,7 +161,15 @@ double num(std::string s) {
 }
 
 // read_parameter (OCFD_readpara.f90:3-200): namelist /control_opencfd/
-bool read_deck(const std::string& path, ocfd_params& p, std::string& err) {
+// ANA_Number and ANA_Para(100, 10) of /control_opencfd/ (OCFD_readpara.f90:12,21,58-59),
+// column-major like the Fortran array: entry m is para[100*m .. 100*m+99] =
+// (code, step interval, data(1:50), ...).
+struct AnaDeck {
+  int number = 0;
+  std::vector<double> para = std::vector<double>(1000, 0.0);
+};
+
+bool read_deck(const std::string& path, ocfd_params& p, std::string& err, AnaDeck* ana = nullptr) {
   std::ifstream is(path);
   if (!is) {
     err = "cannot open " + path;
@@ -269,10 +280,215 @@ bool read_deck(const std::string& path, ocfd_params& p, std::string& err) {
       if (comma != std::string::npos) col = std::atoi(sub.substr(comma + 1).c_str()) - 1;
       for (size_t c = 0; c < v.size() && c < 100; c++) p.filter_para[col][c] = num(v[c]);
     }
-    // npx0/npy0/npz0, ANA_Number/ANA_Para: one rank here; analysis is done by the host tools
+    else if (key == "ANA_NUMBER" && ana) {
+      ana->number = (int)num(v[0]);
+    } else if (key == "ANA_PARA" && ana) {
+      int r0 = 0, c0 = 0;
+      if (!sub.empty()) {
+        const size_t comma = sub.find(',');
+        const std::string a = sub.substr(0, comma), b = comma == std::string::npos ? "" : sub.substr(comma + 1);
+        if (!a.empty() && a != ":") r0 = std::atoi(a.c_str()) - 1;
+        if (!b.empty() && b != ":") c0 = std::atoi(b.c_str()) - 1;
+      }
+      const int st = r0 + 100 * c0;
+      for (size_t c = 0; c < v.size() && st + (int)c < 1000; c++) ana->para[st + c] = num(v[c]);
+    }
+    // npx0/npy0/npz0: one rank here
+  }
+  if (ana && ana->number > 10) {
+    err = "ANA_Number and NFiltering should <=10";
+    return false;
   }
   return true;
 }
+
+// Fortran Ew.dE2 edit descriptor: 0.ddd...E+xx, right-aligned in w columns.
+std::string fortran_e(double x, int w = 20, int d = 13) {
+  std::string body;
+  if (x == 0.0) {
+    body = "0." + std::string(d, '0') + "E+00";
+  } else {
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.*E", d - 1, std::fabs(x));
+    std::string m(buf);
+    const size_t e = m.find('E');
+    std::string digits = m.substr(0, e);
+    digits.erase(std::remove(digits.begin(), digits.end(), '.'), digits.end());
+    const int ex = std::atoi(m.c_str() + e + 1) + 1;
+    char eb[16];
+    std::snprintf(eb, sizeof(eb), "E%c%02d", ex >= 0 ? '+' : '-', std::abs(ex));
+    body = "0." + digits + eb;
+    if (x < 0) body = "-" + body;
+  }
+  if ((int)body.size() < w) body = std::string(w - body.size(), ' ') + body;
+  return body;
+}
+
+// OCFD_analysis after a step: every entry whose interval divides Istep, with
+// the reference's files (OCFD_ANA.f90:3-31; codes OCFD_parameters.f90:36-37):
+//   100 ana_time_average  means of d,u,v,w,T (restart from opencfd.dat.average);
+//                         every data(1) steps OCFD%08d.dat.average
+//   101 ana_getQ          Q-%07d.dat, nz records of nx*ny
+//   102 ana_box           a row of statistics.dat, '(20(E20.13E2))'
+//   103 ana_savedata      planes (1 YZ, 2 XZ, 3 XY), points (4), a block (5)
+//   104 Ana_corner        WallUtp-log.dat: (Istep, tt), then u_t, T, p_w
+struct Analysis {
+  ocfd_handle* h;
+  int nx, ny, nz;
+  const AnaDeck& deck;
+  bool avg_started = false;
+
+  static void rec(std::ofstream& os, const void* p, size_t bytes) { write_record(os, p, (uint32_t)bytes); }
+  static std::string head(int istep, double tt) {
+    std::string b(12, '\0');
+    std::memcpy(&b[0], &istep, 4);
+    std::memcpy(&b[4], &tt, 8);
+    return b;
+  }
+  bool block(int ib, int ie, int jb, int je, int kb, int ke, std::vector<std::vector<double>>& out) {
+    const size_t m = (size_t)(ie - ib + 1) * (je - jb + 1) * (ke - kb + 1);
+    out.assign(5, std::vector<double>(m));
+    double* o[5] = {out[0].data(), out[1].data(), out[2].data(), out[3].data(), out[4].data()};
+    return ocfd_gpu_download_block(h, ib, ie, jb, je, kb, ke, o) == OCFD_OK;
+  }
+  int run(int istep, double tt) {
+    for (int e = 0; e < deck.number; e++) {
+      const double* P = &deck.para[100 * e];
+      const int code = (int)std::lround(P[0]), every = (int)std::lround(P[1]);
+      const double* data = P + 2;
+      if (every <= 0 || istep % every != 0) continue;
+      if (code == 100) {
+        if (!time_average(istep, tt, data)) return 1;
+      } else if (code == 101) {
+        std::vector<double> q((size_t)nx * ny * nz);
+        if (ocfd_gpu_ana_q(h, q.data()) != OCFD_OK) return 1;
+        char name[32];
+        std::snprintf(name, sizeof(name), "Q-%07d.dat", istep);
+        std::ofstream os(name, std::ios::binary);
+        for (int k = 0; k < nz; k++) rec(os, q.data() + (size_t)k * nx * ny, (size_t)nx * ny * 8);
+      } else if (code == 102) {
+        double row[20];
+        if (ocfd_gpu_ana_box(h, row) != OCFD_OK) return 1;
+        std::ofstream os("statistics.dat", std::ios::app);
+        for (int c = 0; c < 20; c++) os << fortran_e(row[c]);
+        os << "\n";
+      } else if (code == 103) {
+        if (!savedata(istep, tt, data)) return 1;
+      } else if (code == 104) {
+        std::vector<double> out(3 * (size_t)nx);
+        if (ocfd_gpu_ana_corner(h, out.data()) != OCFD_OK) return 1;
+        std::ofstream os("WallUtp-log.dat", std::ios::binary | std::ios::app);
+        const std::string hd = head(istep, tt);
+        rec(os, hd.data(), 12);
+        rec(os, out.data(), out.size() * 8);
+      } else {
+        std::fprintf(stderr, "analysis code %d is not supported\n", code);
+        return 1;
+      }
+    }
+    return 0;
+  }
+  bool time_average(int istep, double tt, const double* data) {
+    const size_t plane = (size_t)nx * ny, n = plane * nz;
+    if (!avg_started) {
+      avg_started = true;
+      std::ifstream is("opencfd.dat.average", std::ios::binary);
+      if (is) {
+        char r1[12];
+        if (!read_record(is, r1, 12)) return false;
+        int k_avg;
+        double t_avg;
+        std::memcpy(&k_avg, r1, 4);
+        std::memcpy(&t_avg, r1 + 4, 8);
+        std::vector<std::vector<double>> m(5, std::vector<double>(n));
+        for (int v = 0; v < 5; v++)
+          for (int k = 0; k < nz; k++)
+            if (!read_record(is, m[v].data() + k * plane, (uint32_t)(plane * 8))) return false;
+        const double* mp[5] = {m[0].data(), m[1].data(), m[2].data(), m[3].data(), m[4].data()};
+        if (ocfd_gpu_upload_average(h, mp, k_avg, t_avg) != OCFD_OK) return false;
+      }
+    }
+    if (ocfd_gpu_ana_time_average(h) != OCFD_OK) return false;
+    const int every_save = (int)std::lround(data[0]);
+    if (every_save > 0 && istep % every_save == 0) {
+      std::vector<std::vector<double>> m(5, std::vector<double>(n));
+      double* mp[5] = {m[0].data(), m[1].data(), m[2].data(), m[3].data(), m[4].data()};
+      int k_avg = 0;
+      double t_avg = 0;
+      if (ocfd_gpu_download_average(h, mp, &k_avg, &t_avg) != OCFD_OK) return false;
+      char name[40];
+      std::snprintf(name, sizeof(name), "OCFD%08d.dat.average", istep);
+      std::ofstream os(name, std::ios::binary);
+      const std::string hd = head(k_avg, t_avg);
+      rec(os, hd.data(), 12);
+      for (int v = 0; v < 5; v++)
+        for (int k = 0; k < nz; k++) rec(os, m[v].data() + k * plane, plane * 8);
+    }
+    (void)tt;
+    return true;
+  }
+  // ana_savedata (OCFD_ANA_savedata.f90:3-196)
+  bool savedata(int istep, double tt, const double* data) {
+    const int kind = (int)std::lround(data[0]);
+    const std::string hd = head(istep, tt);
+    std::vector<std::vector<double>> b;
+    if (kind >= 1 && kind <= 3) {
+      const int points = (int)std::lround(data[1]), band = (int)std::lround(data[2]);
+      const char* tag = kind == 1 ? "YZ" : (kind == 2 ? "XZ" : "XY");
+      for (int ka = 1; ka <= points; ka++) {
+        const int at = (int)std::lround(data[2 + ka]);
+        char name[40];
+        std::snprintf(name, sizeof(name), "savedata-%s%03d.dat", tag, ka);
+        std::ofstream os(name, std::ios::binary | std::ios::app);
+        rec(os, hd.data(), 12);
+        for (int q = at; q < at + band; q++) {
+          const bool ok = kind == 1 ? block(q, q, 1, ny, 1, nz, b)
+                                    : (kind == 2 ? block(1, nx, q, q, 1, nz, b) : block(1, nx, 1, ny, q, q, b));
+          if (!ok) return false;
+          for (auto& v : b) rec(os, v.data(), v.size() * 8);
+        }
+      }
+    } else if (kind == 4) {
+      std::ifstream is("save_points_locations.dat");
+      int m = 0;
+      if (!(is >> m)) return false;
+      std::string rest;
+      std::getline(is, rest);
+      std::vector<std::vector<double>> vals(5, std::vector<double>(m));
+      for (int c = 0; c < m; c++) {
+        std::string line;
+        std::getline(is, line);
+        std::istringstream ls(line);
+        int i = 0, j = 0, k = 0;
+        ls >> i >> j >> k;
+        if (!block(i, i, j, j, k, k, b)) return false;
+        for (int q = 0; q < 5; q++) vals[q][c] = b[q][0];
+      }
+      std::ofstream os("save_points.dat", std::ios::binary | std::ios::app);
+      rec(os, &tt, 8);
+      for (int q = 0; q < 5; q++) rec(os, vals[q].data(), (size_t)m * 8);
+    } else if (kind == 5) {
+      int r[7];
+      for (int c = 0; c < 7; c++) r[c] = (int)std::lround(data[1 + c]);
+      if (!block(r[0], r[1], r[2], r[3], r[4], r[5], b)) return false;
+      char name[40];
+      std::snprintf(name, sizeof(name), "savedata-block%03d.dat", r[6]);
+      std::ofstream os(name, std::ios::binary | std::ios::app);
+      rec(os, hd.data(), 12);
+      for (auto& v : b) rec(os, v.data(), v.size() * 8);
+    }
+    return true;
+  }
+  // steps until the next step at which some entry runs
+  int next_due(int istep) const {
+    int best = 1 << 30;
+    for (int e = 0; e < deck.number; e++) {
+      const int every = (int)std::lround(deck.para[100 * e + 1]);
+      if (every > 0) best = std::min(best, every - istep % every);
+    }
+    return best;
+  }
+};
 
 int fail(const char* what, int rc, ocfd_handle* h = nullptr) {
   std::fprintf(stderr, "%s failed (%d)%s%s\n", what, rc, h ? ": " : "", h ? ocfd_gpu_last_error(h) : "");
@@ -313,7 +529,8 @@ int main(int argc, char** argv) {
   ocfd_params p;
   ocfd_default_params(&p);
   std::string err;
-  if (!read_deck(deck, p, err)) {
+  AnaDeck ana;
+  if (!read_deck(deck, p, err, &ana)) {
     std::fprintf(stderr, "%s\n", err.c_str());
     return 1;
   }
@@ -392,8 +609,9 @@ int main(int argc, char** argv) {
   auto t0 = std::chrono::steady_clock::now();
   long done = 0;
   const int show = p.istep_show > 0 ? p.istep_show : 1;
+  Analysis an{h, nx, ny, nz, ana};
   while (tt < p.end_time - p.dt * 1e-4 && (max_steps < 0 || done < max_steps)) {
-    int k = show - (istep % show);
+    int k = std::min(show - (istep % show), an.next_due(istep));
     const long left_t = (long)std::ceil((p.end_time - p.dt * 1e-4 - tt) / p.dt);
     if (k > left_t) k = (int)left_t;
     if (max_steps >= 0 && k > max_steps - done) k = (int)(max_steps - done);
@@ -407,6 +625,7 @@ int main(int argc, char** argv) {
     if (rc) return fail("step", rc, h);
     done += k;
     ocfd_gpu_get_time(h, &istep, &tt);
+    if (an.run(istep, tt)) return fail("analysis", 1, h);
     if (istep % show == 0) {
       double E0[3];
       ocfd_gpu_show_flow_msg(h, E0);

@@ -72,3 +72,47 @@ def test_driver_restart_run_matches_oracle(tmp_path):
             ref = interior(o.prim(v))
             assert rel_l2(q[v], ref) < 1e-10, (istep, v)
     o.close()
+
+
+def test_driver_analysis_files_match_python_host(tmp_path):
+    """ANA_Para in the deck: the C++ driver runs OCFD_analysis after each step
+    (Q criterion, statistics.dat, time averages with restart-file output,
+    plane and block savedata) and writes the same bytes as the Python host's
+    analysis schedule over the same library."""
+    from ocfd_b200 import analysis
+    from ocfd_b200.solver import Solver
+
+    subprocess.run(["make", "-s", "host/ocfd_sc"], cwd=PKG, check=True)
+    deck = DECK.replace(" $end", """ ANA_Number=5
+ ANA_Para(1,1)=101, 2
+ ANA_Para(1,2)=102, 1
+ ANA_Para(1,3)=100, 1, 2
+ ANA_Para(1,4)=103, 2, 5, 3, 6, 2, 5, 1, 3, 7
+ ANA_Para(1,5)=103, 2, 3, 2, 1, 4, 9
+ $end""")
+    run_dir, py_dir = tmp_path / "drv", tmp_path / "py"
+    run_dir.mkdir()
+    py_dir.mkdir()
+    (run_dir / "opencfd2.in").write_text(deck)
+    p = read_namelist(str(run_dir / "opencfd2.in"))
+    x, y, z = cases.box_coords(p.nx, p.ny, p.nz)
+    fileio.write_grid(str(run_dir / "OCFD-grid.dat"), GRID1D, x, y, z)
+    prims = cases.tgv_prims(cases.tgv_params(24, ny=20, nz=16, ma=0.3))
+    fileio.write_flow(str(run_dir / "opencfd.dat"), 10, 0.04, prims)
+    r = subprocess.run([os.path.join(PKG, "host", "ocfd_sc"), "--steps", "4"], cwd=run_dir,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+    s = Solver(p)
+    s.init_mesh(*fileio.read_grid(str(run_dir / "OCFD-grid.dat"), GRID1D, p.nx, p.ny, p.nz))
+    s.init3d(prims, 10, 0.04)
+    ana = analysis.Analysis(s, analysis.read_analysis(deck, is_text=True), outdir=str(py_dir))
+    for _ in range(4):
+        s.step(1)
+        ana.run()
+    s.close()
+    names = sorted(f.name for f in py_dir.iterdir())
+    assert "Q-0000012.dat" in names and "statistics.dat" in names and "OCFD00000012.dat.average" in names
+    assert "savedata-block007.dat" in names and "savedata-XY001.dat" in names
+    for name in names:
+        assert (run_dir / name).read_bytes() == (py_dir / name).read_bytes(), name

@@ -78,10 +78,14 @@ struct Patches {
   int box[16][6];
 };
 
-__global__ void k_rh_sensor1(Grid G, double p00, const double* d, const double* T, double* rh) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G.n; t += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    decode(G, t, i, j, k);
+// one thread a point, 32 x 8 points of a plane a block (no index decoding)
+__global__ void __launch_bounds__(256) k_rh_sensor1(Grid G, double p00, const double* d, const double* T,
+                                                    double* rh) {
+  {
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31) + 1;
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 5) + 1;
+    const int k = blockIdx.z + 1;
+    if (i > G.nx || j > G.ny) return;
     const long long c = G.ih(i, j, k);
     auto P = [&](long long h) -> double { return p00 * d[h] * T[h]; };
     double r = 0.0;
@@ -167,7 +171,7 @@ cudaError_t launch_rhybrid(const Grid& g, const Phys& ph, const DCoef& dc, const
                            const double* hp, cudaStream_t st) {
   const double p00 = 1.0 / (ph.gamma * ph.ma * ph.ma);
   if (sensor == 1) {
-    k_rh_sensor1<<<148 * 8, 256, 0, st>>>(g, p00, d, T, rh);
+    k_rh_sensor1<<<dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz), 256, 0, st>>>(g, p00, d, T, rh);
   } else {
     double* p = scratch;
     double* part = scratch + g.nh;

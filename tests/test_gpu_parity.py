@@ -244,6 +244,26 @@ def test_mixed_precision_close_to_fp64():
     assert abs(eb[1] - ea[1]) / ea[1] < 1e-6
 
 
+@pytest.mark.parametrize("bc", [BC_USER_DEF, BC_BLUNT2D])
+def test_mixed_precision_curvilinear_close_to_fp64(bc):
+    """Mixed precision on the body-fitted grid with wall BCs and ghost cells: the
+    FP32 copies (d, and u,v,w,T interleaved) are refreshed after every stage's
+    BC, so the mixed run stays at FP32 rounding distance from FP64."""
+    p, X, prims = curvilinear_case(bc=bc)
+    pm, _, _ = curvilinear_case(bc=bc)
+    pm.precision = 1
+    a, b = Solver(p), Solver(pm)
+    for s in (a, b):
+        s.init_mesh(*X)
+        s.init3d(prims)
+        s.step(5)
+    fa, fb = a.download_f(), b.download_f()
+    assert np.all(np.isfinite(fb))
+    assert rel_l2(fb, fa) < 1e-5
+    a.close()
+    b.close()
+
+
 def test_mixed_step_leaves_consistent_fp64_primitives():
     """Mixed precision on a periodic box: stages 1 and 2 of a step skip the FP64
     d,u,v,w (only their FP32 copies are read before stage 3), so after every

@@ -445,6 +445,9 @@ def run_ours(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "bytes_per_point": model[dom],
                          "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+                         # algorithmic bytes / measured HBM bandwidth, every kernel of the step
+                         "hbm_frac_by_kernel": {k: round(model[k] * n / (groups[k] / 3.0 * 1e-3) / 1e9 / peak, 3)
+                                                for k in groups if groups[k] > 0},
                          "note": ("the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM "
                                   "bound: ncu pipe and DRAM fractions per kernel in "
                                   "profiles/kernels_tgv192_omp6_char.md")},

@@ -293,17 +293,19 @@ template cudaError_t launch_visc_grad_batch<float, float>(const BatchTab<ViscArg
 // Flux difference of the three sweeps into du (OCFD_inviscous.f90:106-108,
 // :144-146, :182-184; OCFD_inviscous_character.f90:58-62, :98-102, :137-141),
 // plus the mass force (:189-201).
-template <bool CHAR, typename R>
+// IX: index type of the face / viscous-flux offsets (int when every offset fits,
+// measured 6% faster on the FP32 tail; long long otherwise).
+template <bool CHAR, typename R, typename IX = long long>
 __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k, R du[5]) {
   const Grid& G = a.g;
   const int lc[3] = {i, j, k};
-  long long f1[3], f0[3];
+  IX f1[3], f0[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const int l = lc[d];
     const int lm = (l == 1 && a.fper[d]) ? G.len(d) : l - 1;
-    f1[d] = G.face(d, l, i, j, k);
-    f0[d] = G.face(d, lm, i, j, k);
+    f1[d] = (IX)G.face(d, l, i, j, k);
+    f0[d] = (IX)G.face(d, lm, i, j, k);
   }
   const R ajac = R(a.ajac[G.ih(i, j, k)]);
 #pragma unroll
@@ -312,7 +314,7 @@ __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       const R* H = a.hf[d];
-      const long long fs = a.fs[d];
+      const IX fs = (IX)a.fs[d];
       if (!CHAR && !OCFD_FV_SUMMED)
         dd[d] = (H[f1[d] + m * fs] - H[f0[d] + m * fs] + H[f1[d] + (5 + m) * fs] - H[f0[d] + (5 + m) * fs]) *
                 R(a.h_1[d]);
@@ -337,14 +339,14 @@ __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k
 // du_viscous part 2 (OCFD_viscous.f90:266-282): du(:,:,:,m+1) +=
 // (d/dxi Ev1 + d/deta Ev2 + d/dzeta Ev3) * Ajac, periodic directions read
 // the wrapped neighbours (the reference's exchange_boundary_x/y/z of Ev).
-template <typename R>
+template <typename R, typename IX = long long>
 __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int k, R du[5]) {
   const Grid& G = a.g;
   const int cd8 = a.ph.scheme_vis == 6;
-  const long long o = G.ii(i, j, k);
-  const long long n = G.n;
+  const IX o = (IX)G.ii(i, j, k);
+  const IX n = (IX)G.n;
   const int lc[3] = {i, j, k};
-  const long long is[3] = {1, (long long)G.nx, (long long)G.nx * G.ny};
+  const IX is[3] = {1, (IX)G.nx, (IX)G.nx * (IX)G.ny};
   const R ajac = R(a.ajac[G.ih(i, j, k)]);
   // points within 4 of a periodic end read wrapped neighbours (the Ev arrays
   // carry no halo); the others address their neighbours directly
@@ -354,18 +356,18 @@ __device__ __forceinline__ void visc_div(const UpdArgs<R>& a, int i, int j, int 
   V4<R> s[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    const R* E = a.ev + ((long long)d * n + o) * 4;
+    const R* E = a.ev + ((IX)d * n + o) * 4;
     const int l = lc[d], nn = G.len(d);
     const int per = a.ph.periodic[d];
-    const long long st = is[d] * 4;
+    const IX st = is[d] * 4;
     if (!wz[d]) {
-      auto at = [&](int off) -> V4<R> { return ldg4(E + (long long)off * st); };
+      auto at = [&](int off) -> V4<R> { return ldg4(E + (IX)off * st); };
       s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
     } else {
       auto at = [&](int off) -> V4<R> {
         int l2 = l + off;
         l2 = l2 < 1 ? l2 + nn : (l2 > nn ? l2 - nn : l2);
-        return ldg4(E + (long long)(l2 - l) * st);
+        return ldg4(E + (IX)(l2 - l) * st);
       };
       s[d] = d0<R>(at, l, nn, per, cd8, d0c<R>(a.dc, d));
     }
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(256) k_visc_div(UpdArgs<R> a) {
 }
 
 // The fused stage tail.
-template <bool CHAR, bool VISC, bool FUSEBC, typename R>
+template <bool CHAR, bool VISC, bool FUSEBC, typename R, typename IX = long long>
 __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, const int by, const int bz) {
   const Grid& G = a.g;
   const int i = bx * 32 + (threadIdx.x & 31) + 1;
@@ -513,8 +515,8 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
   const int k = bz + 1;
   if (i > G.nx || j > G.ny) return;
   R du[5];
-  inv_div<CHAR>(a, i, j, k, du);
-  if (VISC) visc_div(a, i, j, k, du);
+  inv_div<CHAR, R, IX>(a, i, j, k, du);
+  if (VISC) visc_div<R, IX>(a, i, j, k, du);
   const long long o = G.ii(i, j, k);
   const long long n = G.n;
   double dd[5];
@@ -560,15 +562,15 @@ __device__ __forceinline__ void fused_body(const UpdArgs<R>& a, const int bx, co
   }
 }
 
-template <bool CHAR, bool VISC, bool FUSEBC, typename R, bool SLAB>
+template <bool CHAR, bool VISC, bool FUSEBC, typename R, bool SLAB, typename IX>
 __global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused(UpdArgs<R> a, SlabOrder so) {
   if (!SLAB) {
-    fused_body<CHAR, VISC, FUSEBC, R>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+    fused_body<CHAR, VISC, FUSEBC, R, IX>(a, blockIdx.x, blockIdx.y, blockIdx.z);
     return;
   }
   int bx, by, bz;
   if (!slab_decode(so, a.g.nz, bx, by, bz)) return;
-  fused_body<CHAR, VISC, FUSEBC, R>(a, bx, by, bz);
+  fused_body<CHAR, VISC, FUSEBC, R, IX>(a, bx, by, bz);
 }
 template <bool CHAR, bool VISC, bool FUSEBC, typename R>
 __global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused_batch(BatchTab<UpdArgs<R>> b) {
@@ -598,12 +600,20 @@ cudaError_t launch_fused(const UpdArgs<R>& a, cudaStream_t st) {
   const SlabOrder so = slab_order(a.g);
   const bool slab = so.sy != so.gy;
   const dim3 grid = slab ? slab_grid(so, a.g.nz) : update_dims(a.g);
+  // FP32 tails index faces and viscous fluxes in 32 bits when every offset fits
+  long long fmax = 0;
+  for (int d = 0; d < 3; d++) fmax = std::max(fmax, a.fs[d]);
+  const bool i32 = sizeof(R) == 4 && 12LL * a.g.n < 2147483647LL && 10LL * fmax < 2147483647LL;
 #define OCFD_FUSED(C, V, B)                                                     \
   if (!!a.chr == C && !!a.visc == V && !!a.fuse_bc == B) {                      \
-    if (slab)                                                                   \
-      k_fused<C, V, B, R, true><<<grid, 256, 0, st>>>(a, so);                   \
+    if (i32 && slab)                                                            \
+      k_fused<C, V, B, R, true, int><<<grid, 256, 0, st>>>(a, so);              \
+    else if (i32)                                                               \
+      k_fused<C, V, B, R, false, int><<<grid, 256, 0, st>>>(a, so);             \
+    else if (slab)                                                              \
+      k_fused<C, V, B, R, true, long long><<<grid, 256, 0, st>>>(a, so);        \
     else                                                                        \
-      k_fused<C, V, B, R, false><<<grid, 256, 0, st>>>(a, so);                  \
+      k_fused<C, V, B, R, false, long long><<<grid, 256, 0, st>>>(a, so);       \
   }
   OCFD_FUSED(false, false, false)
   OCFD_FUSED(false, false, true)

@@ -691,6 +691,20 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           // projected once -- and only the three points of the monotonicity test
           // are projected (results move by rounding only).  Components that fail
           // the test are queued for the block-wide limiter pass below.
+          // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
+          // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
+          auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
+            const R A = V2 * f0 - u1 * f1 - v1 * f2 - w1 * f3 + f4;
+            const R B = un * f0 - n1 * f1 - n2 * f2 - n3 * f3;
+            c[0] = f0 - KK * A;
+            c[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul * f0;
+            c[2] = m1 * f1 + m2 * f2 + m3 * f3 - um * f0;
+            c[3] = KK1 * A + X1 * B;
+            c[4] = KK1 * A - X1 * B;
+          };
+          auto proj5 = [&](int vb, int q, R* c) {
+            proj5v(W(vb, q), W(vb + 1, q), W(vb + 2, q), W(vb + 3, q), W(vb + 4, q), c);
+          };
           {
             R G[5];
 #pragma unroll
@@ -700,12 +714,15 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               for (int q = 6; q >= 0; q--) acc = acc + oa[7 - q] * W(v, q);
               G[v] = acc;
             }
+            proj5v(G[0], G[1], G[2], G[3], G[4], dP);
+            R pa[5], pb[5], pc[5];
+            proj5(0, 2, pa);
+            proj5(0, 3, pb);
+            proj5(0, 4, pc);
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              dP[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
-              const R vm1 = proj_row(r, 0, 2), v0 = proj_row(r, 0, 3), vp1 = proj_row(r, 0, 4);
-              const R mp = v0 + minmod2((vp1 - v0), kap * (v0 - vm1));
-              dfl |= ((dP[r] - v0) * (dP[r] - mp) >= ep ? 1u : 0u) << r;
+              const R mp = pb[r] + minmod2((pc[r] - pb[r]), kap * (pb[r] - pa[r]));
+              dfl |= ((dP[r] - pb[r]) * (dP[r] - mp) >= ep ? 1u : 0u) << r;
             }
           }
           {
@@ -717,12 +734,15 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               for (int q = 1; q <= 7; q++) acc = acc + oa[q] * W(5 + v, q);
               G[v] = acc;
             }
+            proj5v(G[0], G[1], G[2], G[3], G[4], dM);
+            R pa[5], pb[5], pc[5];
+            proj5(5, 3, pa);
+            proj5(5, 4, pb);
+            proj5(5, 5, pc);
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              dM[r] = L[r][0] * G[0] + L[r][1] * G[1] + L[r][2] * G[2] + L[r][3] * G[3] + L[r][4] * G[4];
-              const R v0 = proj_row(r, 5, 3), v1 = proj_row(r, 5, 4), v2 = proj_row(r, 5, 5);
-              const R mp = v1 + minmod2((v0 - v1), kap * (v1 - v2));
-              dfl |= ((dM[r] - v1) * (dM[r] - mp) >= ep ? 1u : 0u) << (5 + r);
+              const R mp = pb[r] + minmod2((pa[r] - pb[r]), kap * (pb[r] - pc[r]));
+              dfl |= ((dM[r] - pb[r]) * (dM[r] - mp) >= ep ? 1u : 0u) << (5 + r);
             }
           }
           if (dfl) {

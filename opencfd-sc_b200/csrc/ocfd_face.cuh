@@ -675,6 +675,20 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           if (r == 1 || r == 2) return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3;
           return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3 + L[r][4] * W(vb + 4, q);
         };
+        // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
+        // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
+        auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
+          const R A = V2 * f0 - u1 * f1 - v1 * f2 - w1 * f3 + f4;
+          const R B = un * f0 - n1 * f1 - n2 * f2 - n3 * f3;
+          c[0] = f0 - KK * A;
+          c[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul * f0;
+          c[2] = m1 * f1 + m2 * f2 + m3 * f3 - um * f0;
+          c[3] = KK1 * A + X1 * B;
+          c[4] = KK1 * A - X1 * B;
+        };
+        auto proj5 = [&](int vb, int q, R* c) {
+          proj5v(W(vb, q), W(vb + 1, q), W(vb + 2, q), W(vb + 3, q), W(vb + 4, q), c);
+        };
         R h0[5];
         if (SCHEME == SCH_OMP6 && inner) {
           // OMP6, interior face: the linear part of hh_OMP6P/M (OCFD_Schemes_1.f90:211,244) is
@@ -691,20 +705,6 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           // projected once -- and only the three points of the monotonicity test
           // are projected (results move by rounding only).  Components that fail
           // the test are queued for the block-wide limiter pass below.
-          // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
-          // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
-          auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
-            const R A = V2 * f0 - u1 * f1 - v1 * f2 - w1 * f3 + f4;
-            const R B = un * f0 - n1 * f1 - n2 * f2 - n3 * f3;
-            c[0] = f0 - KK * A;
-            c[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul * f0;
-            c[2] = m1 * f1 + m2 * f2 + m3 * f3 - um * f0;
-            c[3] = KK1 * A + X1 * B;
-            c[4] = KK1 * A - X1 * B;
-          };
-          auto proj5 = [&](int vb, int q, R* c) {
-            proj5v(W(vb, q), W(vb + 1, q), W(vb + 2, q), W(vb + 3, q), W(vb + 4, q), c);
-          };
           {
             R G[5];
 #pragma unroll
@@ -843,9 +843,17 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             R q[5][8];
             constexpr int LO = Stencil<SCHEME>::PLO, HI = Stencil<SCHEME>::PHI;
 #pragma unroll
-            for (int s = -3; s <= 4; s++)
+            for (int s = -3; s <= 4; s++) {
+#if OCFD_FEWER_DIVS
+              R c[5] = {R(0), R(0), R(0), R(0), R(0)};
+              if (s >= LO && s <= HI) proj5(0, s + 3, c);
+#pragma unroll
+              for (int r = 0; r < 5; r++) q[r][s + 3] = c[r];
+#else
 #pragma unroll
               for (int r = 0; r < 5; r++) q[r][s + 3] = (s < LO || s > HI) ? R(0) : proj_row(r, 0, s + 3);
+#endif
+            }
             if (ALLIN || inner1) {
 #pragma unroll
               for (int r = 0; r < 5; r++) h0[r] = schemeP<SCHEME>(q[r] + 3, U, ihy);
@@ -859,9 +867,17 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             R q[5][8];
             constexpr int LO = Stencil<SCHEME>::MLO, HI = Stencil<SCHEME>::MHI;
 #pragma unroll
-            for (int s = -3; s <= 4; s++)
+            for (int s = -3; s <= 4; s++) {
+#if OCFD_FEWER_DIVS
+              R c[5] = {R(0), R(0), R(0), R(0), R(0)};
+              if (s >= LO && s <= HI) proj5(5, s + 3, c);
+#pragma unroll
+              for (int r = 0; r < 5; r++) q[r][s + 3] = c[r];
+#else
 #pragma unroll
               for (int r = 0; r < 5; r++) q[r][s + 3] = (s < LO || s > HI) ? R(0) : proj_row(r, 5, s + 3);
+#endif
+            }
             if (ALLIN || inner2) {
 #pragma unroll
               for (int r = 0; r < 5; r++) h0[r] = h0[r] + schemeM<SCHEME>(q[r] + 3, U, ihy);

@@ -980,9 +980,10 @@ static int fused_stage(ocfd_handle* h, int krk, Prof* pf = nullptr) {
     if (rb) return rb;
     CK(launch_bc_refresh(h->g, h->ph, h->f, h->prim, h->st));
     CK(launch_ghost(h->g, h->ph, h->prim, h->st));
+    // FP32 copies: the tail wrote the interior; the boundary planes and ghost
+    // layers the BC changed are converted here, the periodic halos exchanged
+    if (h->mixed) CK(launch_refresh_shell(h->g, h->ph.periodic, h->prim, h->p32[0], h->q32, h->st));
     int r = halo_all(h);
-    if (r) return r;
-    r = refresh_p32(h);
     if (r) return r;
   }
   prof_mark(h, pf, 7);

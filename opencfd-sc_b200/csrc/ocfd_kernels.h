@@ -186,6 +186,8 @@ cudaError_t launch_bc_refresh(const Grid& g, const Phys& ph, double* f, double* 
 // Flow_Ghost_Extent_2nd
 cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], cudaStream_t st);
 // FP32 copies of the primitives
+cudaError_t launch_refresh_shell(const Grid& g, const int periodic[3], double* const prim[5], float* p32, float* q32,
+                                 cudaStream_t st);
 cudaError_t launch_to_f32x4(const double* u, const double* v, const double* w, const double* T, float* dst, long long n,
                             cudaStream_t st);
 cudaError_t launch_to_f32(const double* src, float* dst, long long n, cudaStream_t st);

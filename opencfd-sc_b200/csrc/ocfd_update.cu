@@ -1157,6 +1157,31 @@ cudaError_t launch_ghost(const Grid& g, const Phys& ph, double* const prim[5], c
   return cudaGetLastError();
 }
 
+// FP32 copies of the primitives at the points a boundary condition may have
+// changed after the stage tail wrote them: in every non-periodic direction the
+// boundary plane and the ghost layers beyond it (all other points keep the
+// tail's copies).  Grid: (nxh/32, nyh/8, nzh) threads over the haloed array.
+__global__ void k_refresh_shell(Grid G, int px, int py, int pz, const double* d, const double* u, const double* v,
+                                const double* w, const double* T, float* p32, float4* q32) {
+  const int hi = blockIdx.x * 32 + (threadIdx.x & 31), hj = blockIdx.y * 8 + (threadIdx.x >> 5),
+            hk = blockIdx.z;
+  if (hi >= G.nxh || hj >= G.nyh) return;
+  const int i = hi - LAP + 1, j = hj - LAP + 1, k = hk - LAP + 1;
+  const bool shell = (!px && (i <= 1 || i >= G.nx)) || (!py && (j <= 1 || j >= G.ny)) ||
+                     (!pz && (k <= 1 || k >= G.nz));
+  if (!shell) return;
+  const long long c = (long long)hi + (long long)G.nxh * ((long long)hj + (long long)G.nyh * hk);
+  p32[c] = float(d[c]);
+  q32[c] = make_float4(float(u[c]), float(v[c]), float(w[c]), float(T[c]));
+}
+cudaError_t launch_refresh_shell(const Grid& g, const int periodic[3], double* const prim[5], float* p32, float* q32,
+                                 cudaStream_t st) {
+  if (periodic[0] && periodic[1] && periodic[2]) return cudaSuccess;
+  k_refresh_shell<<<dim3((g.nxh + 31) / 32, (g.nyh + 7) / 8, g.nzh), 256, 0, st>>>(
+      g, periodic[0], periodic[1], periodic[2], prim[0], prim[1], prim[2], prim[3], prim[4], p32,
+      reinterpret_cast<float4*>(q32));
+  return cudaGetLastError();
+}
 __global__ void k_to_f32x4(const double* u, const double* v, const double* w, const double* T, float4* dst,
                            long long n) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)

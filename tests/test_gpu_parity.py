@@ -244,6 +244,30 @@ def test_mixed_precision_close_to_fp64():
     assert abs(eb[1] - ea[1]) / ea[1] < 1e-6
 
 
+@pytest.mark.parametrize("case", ["omp6char-fp64", "omp6char-mixed", "curvilinear-fp64"])
+def test_same_bits_twice(case):
+    """Race check: the same run twice gives the same bits (the limiter queue's
+    entry order depends on atomics, its results must not)."""
+    if case.startswith("omp6char"):
+        p, X, prims = tgv_case(scheme=SCHEME_OMP6, character=1, mixed=case.endswith("mixed"), n=(32, 24, 16))
+    else:
+        p, X, prims = curvilinear_case()
+    out = []
+    for _ in range(2):
+        s = Solver(p)
+        if X is None:
+            s.init_mesh()
+        else:
+            s.init_mesh(*X)
+        s.init3d(prims)
+        s.step(6)
+        out.append(s.download_state())
+        s.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("bc", [BC_USER_DEF, BC_BLUNT2D])
 def test_mixed_precision_curvilinear_close_to_fp64(bc):
     """Mixed precision on the body-fitted grid with wall BCs and ghost cells: the

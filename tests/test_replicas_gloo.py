@@ -35,7 +35,7 @@ def test_replicas_world2():
     import torch.multiprocessing as mp
 
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
     assert out[0][0] == [0, 2, 4, 6, 8] and out[1][0] == [1, 3, 5, 7, 9]

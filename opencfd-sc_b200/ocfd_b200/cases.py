@@ -131,7 +131,7 @@ def hit_prims(n: int, mt: float, ma: float, k0: float = 4.0, seed: int = 2026120
     del dot, kk2
     vel = []
     while comps:
-        vel.append(np.fft.irfftn(comps.pop(0), s=(n, n, n)))
+        vel.append(np.fft.irfftn(comps.pop(0), s=(n, n, n), axes=(0, 1, 2)))
     c_mean = 1.0 / ma
     rms = math.sqrt(float(np.mean(vel[0] ** 2) + np.mean(vel[1] ** 2) + np.mean(vel[2] ** 2)))
     s = mt * c_mean / rms

@@ -403,7 +403,7 @@ __global__ void k_metric_div(long long nh, MetPtrs mp) {
 }
 
 cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* const met[22],
-                        const double span[3][3], cudaStream_t st) {
+                        const double span[3][3], bool jac_given, cudaStream_t st) {
   MetPtrs mp;
   for (int m = 0; m < 22; m++) mp.m[m] = met[m];
   PtrList<double> xyz;
@@ -415,7 +415,9 @@ cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* 
                                        make_double3(span[0][0], span[0][1], span[0][2]),
                                        make_double3(span[1][0], span[1][1], span[1][2]),
                                        make_double3(span[2][0], span[2][1], span[2][2]), met[0], met[1], met[2]);
-  k_jacobian<<<148 * 8, 256, 0, st>>>(g, ph, dc, mp);
+  // Iflag_Gridtype = GRID_AND_JACOBIAN3D: the interior metrics and Jacobian came
+  // with the grid (OCFD_mesh.f90:24-26 skips comput_Jacobian3d)
+  if (!jac_given) k_jacobian<<<148 * 8, 256, 0, st>>>(g, ph, dc, mp);
   PtrList<double> m10;
   m10.n = 10;
   for (int m = 0; m < 10; m++) m10.p[m] = met[3 + m];

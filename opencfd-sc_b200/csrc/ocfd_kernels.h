@@ -214,7 +214,7 @@ cudaError_t launch_gather_box(const Grid& g, const double* src, int ib, int ie, 
                               double* dst, cudaStream_t st);
 cudaError_t launch_metric_nonzero(const Grid& g, double* const met[22], unsigned int* nonzero, cudaStream_t st);
 cudaError_t launch_mesh(const Grid& g, const Phys& ph, const DCoef& dc, double* const met[22],
-                        const double periodic_span[3][3], cudaStream_t st);
+                        const double span[3][3], bool jac_given, cudaStream_t st);
 
 // show_flow_msg / ana_box partial sums (deterministic two-level reduction)
 cudaError_t launch_flow_msg(const Grid& g, const Phys& ph, const double* f, double* const prim[5],

@@ -83,9 +83,12 @@ bool read_flow(const std::string& path, int& istep, double& tt, int nx, int ny, 
   return true;
 }
 
-// OCFD-grid.dat: read_mesh1d / read_mesh2d_plane / read_mesh3d (OCFD_mesh.f90:187-283)
+// OCFD-grid.dat: read_mesh1d / read_mesh2d_plane / read_mesh2d_AxialSymm /
+// read_mesh3d (OCFD_mesh.f90:187-317).  Iflag_Gridtype 31 also reads the ten
+// metric / Jacobian arrays into jac (Akx, Aky, Akz, Aix, Aiy, Aiz, Asx, Asy,
+// Asz, Ajac).
 bool read_grid(const std::string& path, int type, int nx, int ny, int nz, std::vector<double>& X,
-               std::vector<double>& Y, std::vector<double>& Z) {
+               std::vector<double>& Y, std::vector<double>& Z, std::vector<std::vector<double>>& jac) {
   std::ifstream is(path, std::ios::binary);
   if (!is) return false;
   const size_t n = (size_t)nx * ny * nz, plane = (size_t)nx * ny;
@@ -107,7 +110,7 @@ bool read_grid(const std::string& path, int type, int nx, int ny, int nz, std::v
         }
     return true;
   }
-  if (type == OCFD_GRID2D_PLANE) {
+  if (type == OCFD_GRID2D_PLANE || type == OCFD_GRID2D_AXIAL_SYMM) {
     std::vector<double> x2(plane), y2(plane), z1(nz);
     if (!read_record(is, x2.data(), (uint32_t)(plane * 8)) || !read_record(is, y2.data(), (uint32_t)(plane * 8)) ||
         !read_record(is, z1.data(), nz * 8))
@@ -115,16 +118,28 @@ bool read_grid(const std::string& path, int type, int nx, int ny, int nz, std::v
     for (int k = 0; k < nz; k++)
       for (size_t c = 0; c < plane; c++) {
         X[c + plane * k] = x2[c];
-        Y[c + plane * k] = y2[c];
-        Z[c + plane * k] = z1[k];
+        if (type == OCFD_GRID2D_PLANE) {
+          Y[c + plane * k] = y2[c];
+          Z[c + plane * k] = z1[k];
+        } else {
+          // read_mesh2d_AxialSymm (OCFD_mesh.f90:286-317): y2 is R, z1 the angle seta
+          Y[c + plane * k] = y2[c] * std::cos(z1[k]);
+          Z[c + plane * k] = y2[c] * std::sin(z1[k]);
+        }
       }
     return true;
   }
-  if (type == OCFD_GRID3D) {
+  if (type == OCFD_GRID3D || type == OCFD_GRID_AND_JACOBIAN3D) {
     std::vector<double>* A[3] = {&X, &Y, &Z};
     for (int a = 0; a < 3; a++)
       for (int k = 0; k < nz; k++)
         if (!read_record(is, A[a]->data() + plane * k, (uint32_t)(plane * 8))) return false;
+    if (type == OCFD_GRID_AND_JACOBIAN3D) {
+      jac.assign(10, std::vector<double>(n));
+      for (int a = 0; a < 10; a++)
+        for (int k = 0; k < nz; k++)
+          if (!read_record(is, jac[a].data() + plane * k, (uint32_t)(plane * 8))) return false;
+    }
     return true;
   }
   return false;
@@ -511,6 +526,19 @@ int io_selftest(const std::string& dir) {
   return 0;
 }
 
+// Reads OCFD-grid.dat as init_mesh would and writes the expanded coordinates
+// (and, for Iflag_Gridtype 31, the ten metric arrays) as raw float64 to out:
+// a check of the readers that needs no GPU.
+int grid_dump(int type, int nx, int ny, int nz, const std::string& in, const std::string& out) {
+  std::vector<double> X, Y, Z;
+  std::vector<std::vector<double>> jac;
+  if (!read_grid(in, type, nx, ny, nz, X, Y, Z, jac)) return 2;
+  std::ofstream os(out, std::ios::binary);
+  for (const std::vector<double>* a : {&X, &Y, &Z}) os.write((const char*)a->data(), a->size() * 8);
+  for (const auto& a : jac) os.write((const char*)a.data(), a.size() * 8);
+  return os ? 0 : 3;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -521,6 +549,9 @@ int main(int argc, char** argv) {
   for (int a = 1; a < argc; a++) {
     std::string s = argv[a];
     if (s == "--io-selftest" && a + 1 < argc) return io_selftest(argv[++a]);
+    if (s == "--grid-dump" && a + 6 < argc)
+      return grid_dump(std::atoi(argv[a + 1]), std::atoi(argv[a + 2]), std::atoi(argv[a + 3]),
+                       std::atoi(argv[a + 4]), argv[a + 5], argv[a + 6]);
     if (s == "--print-params") print_only = true;
     else if (s == "--deck" && a + 1 < argc) deck = argv[++a];
     else if (s == "--device" && a + 1 < argc) device = std::atoi(argv[++a]);
@@ -565,11 +596,18 @@ int main(int argc, char** argv) {
     rc = ocfd_gpu_init_mesh(h, nullptr, nullptr, nullptr);
   } else {
     std::vector<double> X, Y, Z;
-    if (!read_grid("OCFD-grid.dat", p.iflag_gridtype, nx, ny, nz, X, Y, Z)) {
+    std::vector<std::vector<double>> jac;
+    if (!read_grid("OCFD-grid.dat", p.iflag_gridtype, nx, ny, nz, X, Y, Z, jac)) {
       std::fprintf(stderr, "cannot read OCFD-grid.dat for Iflag_Gridtype %d\n", p.iflag_gridtype);
       return 1;
     }
-    rc = ocfd_gpu_init_mesh(h, X.data(), Y.data(), Z.data());
+    if (jac.empty()) {
+      rc = ocfd_gpu_init_mesh(h, X.data(), Y.data(), Z.data());
+    } else {
+      const double* J[10];
+      for (int a = 0; a < 10; a++) J[a] = jac[a].data();
+      rc = ocfd_gpu_init_mesh_jacobian(h, X.data(), Y.data(), Z.data(), J);
+    }
   }
   if (rc) return fail("init_mesh", rc, h);
   // ---- read_flow_data, or flowfield_init('TGV') (OCFD_flowinit.f90:18-28)

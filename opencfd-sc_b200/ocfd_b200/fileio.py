@@ -7,8 +7,11 @@
   (Istep: int32, tt: real64); then d, u, v, w, T follow, each as nz records of
   nx*ny real64 (one k-plane per record, i fastest).
 - Grid file ``OCFD-grid.dat``: read_mesh1d (x(nx), y(ny), z(nz) as three
-  records), read_mesh2d_plane (x(nx,ny), y(nx,ny), z(nz)) and read_mesh3d (x,
-  y, z as nz plane records each) (OCFD_mesh.f90:187-283).
+  records), read_mesh2d_plane (x(nx,ny), y(nx,ny), z(nz)),
+  read_mesh2d_AxialSymm (x(nx,ny), R(nx,ny), seta(nz); y = R cos(seta),
+  z = R sin(seta)) and read_mesh3d (x, y, z as nz plane records each, followed
+  for Iflag_Gridtype 31 by Akx, Aky, Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Ajac in
+  the same layout) (OCFD_mesh.f90:187-317).
 
 Arrays are numpy (nz, ny, nx) C-order, i.e. the Fortran (nx, ny, nz) layout.
 """
@@ -16,7 +19,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .params import GRID1D, GRID2D_PLANE, GRID3D
+from .params import GRID1D, GRID2D_AXIAL_SYMM, GRID2D_PLANE, GRID3D, GRID_AND_JACOBIAN3D
 
 _MARK = np.dtype("<i4")
 
@@ -67,28 +70,45 @@ def read_flow(path: str, nx: int, ny: int, nz: int):
     return istep, tt, prims
 
 
-def write_grid(path: str, gridtype: int, x, y, z) -> None:
-    """OCFD-grid.dat in the layout read_mesh* expect for this Iflag_Gridtype."""
+def _write_planes(fh, a) -> None:
+    a = np.ascontiguousarray(a, dtype="<f8")
+    for k in range(a.shape[0]):
+        _write_record(fh, a[k].tobytes())
+
+
+def _read_planes(fh, nx: int, ny: int, nz: int) -> np.ndarray:
+    a = np.empty((nz, ny, nx))
+    for k in range(nz):
+        a[k] = np.frombuffer(_read_record(fh, nx * ny * 8), dtype="<f8").reshape(ny, nx)
+    return a
+
+
+def write_grid(path: str, gridtype: int, x, y, z, jac=None) -> None:
+    """OCFD-grid.dat in the layout read_mesh* expect for this Iflag_Gridtype.
+    GRID1D: x(nx), y(ny), z(nz); GRID2D_PLANE: x, y (ny, nx) and z(nz);
+    GRID2D_AXIAL_SYMM: x, R (ny, nx) and seta(nz); GRID3D: x, y, z (nz, ny, nx);
+    GRID_AND_JACOBIAN3D: the same plus jac, the ten (nz, ny, nx) arrays Akx, Aky,
+    Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Ajac."""
     with open(path, "wb") as fh:
-        if gridtype == GRID1D:
+        if gridtype in (GRID1D, GRID2D_PLANE, GRID2D_AXIAL_SYMM):
             for a in (x, y, z):
                 _write_record(fh, np.ascontiguousarray(a, dtype="<f8").tobytes())
-        elif gridtype == GRID2D_PLANE:
-            _write_record(fh, np.ascontiguousarray(x, dtype="<f8").tobytes())
-            _write_record(fh, np.ascontiguousarray(y, dtype="<f8").tobytes())
-            _write_record(fh, np.ascontiguousarray(z, dtype="<f8").tobytes())
-        elif gridtype == GRID3D:
+        elif gridtype in (GRID3D, GRID_AND_JACOBIAN3D):
             for a in (x, y, z):
-                a = np.ascontiguousarray(a, dtype="<f8")
-                for k in range(a.shape[0]):
-                    _write_record(fh, a[k].tobytes())
+                _write_planes(fh, a)
+            if gridtype == GRID_AND_JACOBIAN3D:
+                if jac is None or len(jac) != 10:
+                    raise ValueError("Iflag_Gridtype 31 needs the ten metric / Jacobian arrays")
+                for a in jac:
+                    _write_planes(fh, a)
         else:
             raise ValueError(f"Iflag_Gridtype {gridtype} has no grid file")
 
 
 def read_grid(path: str, gridtype: int, nx: int, ny: int, nz: int):
     """Read OCFD-grid.dat and expand it to three (nz, ny, nx) coordinate arrays
-    (what init_mesh passes on to the Jacobian)."""
+    (what init_mesh passes on to the Jacobian); for GRID_AND_JACOBIAN3D a fourth
+    item, the list of the ten metric / Jacobian arrays, follows."""
     with open(path, "rb") as fh:
         if gridtype == GRID1D:
             x = np.frombuffer(_read_record(fh, nx * 8), dtype="<f8")
@@ -96,20 +116,24 @@ def read_grid(path: str, gridtype: int, nx: int, ny: int, nz: int):
             z = np.frombuffer(_read_record(fh, nz * 8), dtype="<f8")
             Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
             return X.copy(), Y.copy(), Z.copy()
-        if gridtype == GRID2D_PLANE:
+        if gridtype in (GRID2D_PLANE, GRID2D_AXIAL_SYMM):
             x2 = np.frombuffer(_read_record(fh, nx * ny * 8), dtype="<f8").reshape(ny, nx)
             y2 = np.frombuffer(_read_record(fh, nx * ny * 8), dtype="<f8").reshape(ny, nx)
             z1 = np.frombuffer(_read_record(fh, nz * 8), dtype="<f8")
             X = np.broadcast_to(x2, (nz, ny, nx)).copy()
-            Y = np.broadcast_to(y2, (nz, ny, nx)).copy()
-            Z = np.broadcast_to(z1[:, None, None], (nz, ny, nx)).copy()
+            if gridtype == GRID2D_PLANE:
+                Y = np.broadcast_to(y2, (nz, ny, nx)).copy()
+                Z = np.broadcast_to(z1[:, None, None], (nz, ny, nx)).copy()
+            else:
+                # read_mesh2d_AxialSymm (OCFD_mesh.f90:286-317): y horizontal, z up,
+                # seta the angle from the y axis
+                Y = y2[None, :, :] * np.cos(z1)[:, None, None]
+                Z = y2[None, :, :] * np.sin(z1)[:, None, None]
             return X, Y, Z
-        if gridtype == GRID3D:
-            out = []
-            for _ in range(3):
-                a = np.empty((nz, ny, nx))
-                for k in range(nz):
-                    a[k] = np.frombuffer(_read_record(fh, nx * ny * 8), dtype="<f8").reshape(ny, nx)
-                out.append(a)
-            return tuple(out)
+        if gridtype in (GRID3D, GRID_AND_JACOBIAN3D):
+            out = [_read_planes(fh, nx, ny, nz) for _ in range(3)]
+            if gridtype == GRID3D:
+                return tuple(out)
+            jac = [_read_planes(fh, nx, ny, nz) for _ in range(10)]
+            return out[0], out[1], out[2], jac
     raise ValueError(f"Iflag_Gridtype {gridtype} has no grid file")

@@ -887,7 +887,13 @@ static void jac_ghost_extent_2nd(ocfd_oracle* o) {
  * otherwise interior coordinates as read by read_mesh1d/2d_plane/3d. */
 static void jac_ghost_user(ocfd_oracle* o);
 
-void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const double* z) {
+/* init_mesh (OCFD_mesh.f90:1-58).  jac == NULL: the metrics and Jacobian are
+ * computed from the coordinates (comput_Jacobian3d, :24-26); otherwise jac
+ * holds the interior Akx, Aky, Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Ajac read
+ * from the grid file (Iflag_Gridtype = GRID_AND_JACOBIAN3D, read_mesh3d :187-217)
+ * and only their halos, ghost values and the /Ajac copies are formed. */
+static void init_mesh_common(ocfd_oracle* o, const double* x, const double* y, const double* z,
+                             const double* const jac[10]) {
   double** M = o->met;
   const double PI = 3.1415926535897932;
   for (int k = 1; k <= o->nz; k++)
@@ -908,7 +914,14 @@ void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const doubl
   orc_exchange_xyz(o, M[OCFD_M_AYY]);
   orc_exchange_xyz(o, M[OCFD_M_AZZ]);
   updata_axyz_periodic(o);
-  comput_jacobian3d(o);
+  if (jac == NULL) {
+    comput_jacobian3d(o);
+  } else {
+    for (int m = 0; m < 10; m++)
+      for (int k = 1; k <= o->nz; k++)
+        for (int j = 1; j <= o->ny; j++)
+          for (int i = 1; i <= o->nx; i++) M[OCFD_M_AKX + m][IH(o, i, j, k)] = jac[m][I3(o, i, j, k)];
+  }
   for (int m = OCFD_M_AKX; m <= OCFD_M_AJAC; m++) orc_exchange_xyz(o, M[m]);
   /* Jac_Ghost_boundary: OCFD_GhostCell.f90:1-7 */
   jac_ghost_extent_1st(o);
@@ -918,6 +931,15 @@ void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const doubl
     double J = M[OCFD_M_AJAC][h];
     for (int m = 0; m < 9; m++) M[OCFD_M_AKX1 + m][h] = M[OCFD_M_AKX + m][h] / J;
   }
+}
+
+void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const double* z) {
+  init_mesh_common(o, x, y, z, NULL);
+}
+
+void orc_init_mesh_jacobian(ocfd_oracle* o, const double* x, const double* y, const double* z,
+                            const double* const jac[10]) {
+  init_mesh_common(o, x, y, z, jac);
 }
 
 /* Jac_Ghost_Userdef: OCFD_GhostCell_UserDef.f90:4-11 with Jac_Ghost_Sweptcorner

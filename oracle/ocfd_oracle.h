@@ -47,6 +47,11 @@ void orc_set_time(ocfd_oracle* o, int istep, double tt);
 
 /* init_mesh; x,y,z interior coordinates (Fortran order) or NULL for 'box'. */
 void orc_init_mesh(ocfd_oracle* o, const double* x, const double* y, const double* z);
+/* init_mesh for Iflag_Gridtype = GRID_AND_JACOBIAN3D: jac = interior Akx, Aky,
+ * Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Ajac from the grid file (no
+ * comput_Jacobian3d, OCFD_mesh.f90:24-26). */
+void orc_init_mesh_jacobian(ocfd_oracle* o, const double* x, const double* y, const double* z,
+                            const double* const jac[10]);
 /* init3d from interior primitives + the initial OCFD_bc. */
 void orc_init3d(ocfd_oracle* o, const double* const prims[5]);
 

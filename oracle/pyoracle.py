@@ -49,6 +49,7 @@ def lib() -> C.CDLL:
         L.orc_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_int), dp]
         L.orc_set_time.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_init_mesh.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_init_mesh_jacobian.argtypes = [C.c_void_p, dp, dp, dp, dp * 10]
         L.orc_init3d.argtypes = [C.c_void_p, dp * 5]
         for name in ["orc_halo_prims", "orc_comput_rhybrid", "orc_du_inviscous", "orc_du_inviscous_character",
                      "orc_du_viscous", "orc_bc", "orc_filtering"]:
@@ -133,12 +134,17 @@ class Oracle:
         return [self.metric(m) for m in range(N_METRICS)]
 
     # ---- operations
-    def init_mesh(self, x=None, y=None, z=None):
+    def init_mesh(self, x=None, y=None, z=None, jac=None):
         if x is None:
             lib().orc_init_mesh(self.h, None, None, None)
-        else:
-            xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+            return
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        if jac is None:
             lib().orc_init_mesh(self.h, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]))
+        else:
+            js = [np.ascontiguousarray(a, dtype=np.float64) for a in jac]
+            lib().orc_init_mesh_jacobian(self.h, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]),
+                                         (C.POINTER(C.c_double) * 10)(*[_dp(a) for a in js]))
 
     def init3d(self, prims):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in prims]

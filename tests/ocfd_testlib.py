@@ -114,3 +114,36 @@ def boundary_layer_case(kind="bl", n=(24, 20, 8), ghost=False, tw=-1.0, pert=Tru
     tm, fait = bclayer.time_factor(3, rng)
     data = bclayer.BcLayerData(inlet=inlet, pertb=pertb, beta=20.0 if pert else 0.0, tm=tm, fait=fait)
     return p, (X, Y, Z), prims, data
+
+
+def annulus_case(nx=24, ny=16, nz=20):
+    """Periodic annular duct in axisymmetric form: i axial (periodic, length 2),
+    j radial (R from 0.5 to 1.5, slightly curved walls), k the full circle of
+    angles (periodic, no span shift: the angle wraps).  Uniform axial flow with
+    a smooth perturbation; no boundary condition on the radial faces."""
+    from ocfd_b200.params import BC_NONE, GRID2D_AXIAL_SYMM, default_params
+
+    p = default_params()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.iperiodic[0], p.iperiodic[1], p.iperiodic[2] = 1, 0, 1
+    p.periodic_span[0][0] = 2.0
+    p.iflag_gridtype = GRID2D_AXIAL_SYMM
+    p.ibc = BC_NONE
+    p.scheme_invis = SCHEME_WENO7
+    p.if_scheme_character = 1
+    p.flux_splitting = SPLIT_SW
+    p.ma, p.re, p.pr, p.gamma = 0.5, 1000.0, 0.7, 1.4
+    p.dt = 1e-3
+    p.hybrid_para[3] = 0.0
+    i = np.arange(1, nx + 1)[None, :]
+    j = np.arange(ny)[:, None]
+    x2 = 2.0 * i / nx + 0.0 * j
+    r2 = 0.5 + j / (ny - 1.0) + 0.05 * np.sin(np.pi * i / nx) * (j / (ny - 1.0))
+    seta = 2.0 * np.pi * np.arange(nz) / nz
+    kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    d = 1.0 + 0.02 * np.cos(2 * np.pi * ii / nx)
+    u = 1.0 + 0.05 * np.sin(2 * np.pi * ii / nx) * np.cos(2 * np.pi * kk / nz)
+    v = 0.03 * np.sin(np.pi * jj / ny) * np.sin(2 * np.pi * kk / nz)
+    w = 0.02 * np.cos(2 * np.pi * ii / nx)
+    T = 1.0 + 0.01 * np.cos(np.pi * jj / ny)
+    return p, (x2, r2, seta), [d, u, v, w, T]

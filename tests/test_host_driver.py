@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from ocfd_b200 import fileio
-from ocfd_b200.params import GRID1D, GRID2D_PLANE, GRID3D, read_namelist, set_parameters_py
+from ocfd_b200.params import (GRID1D, GRID2D_AXIAL_SYMM, GRID2D_PLANE, GRID3D, GRID_AND_JACOBIAN3D, read_namelist,
+                              set_parameters_py)
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
@@ -72,23 +73,67 @@ def test_flow_file_round_trip(tmp_path):
         fileio.read_flow(path, 6, 5, 6)
 
 
-@pytest.mark.parametrize("gridtype", [GRID1D, GRID2D_PLANE, GRID3D])
-def test_grid_file_round_trip(tmp_path, gridtype):
-    nx, ny, nz = 6, 5, 4
+def _grid_case(gridtype, nx=6, ny=5, nz=4):
+    """Grid-file contents (x, y, z[, jac]) of a type and the expanded (nz, ny, nx)
+    arrays init_mesh receives."""
     rng = np.random.default_rng(gridtype)
+    jac = None
     if gridtype == GRID1D:
         x, y, z = rng.normal(size=nx), rng.normal(size=ny), rng.normal(size=nz)
         Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    elif gridtype == GRID2D_PLANE:
+    elif gridtype in (GRID2D_PLANE, GRID2D_AXIAL_SYMM):
         x, y, z = rng.normal(size=(ny, nx)), rng.normal(size=(ny, nx)), rng.normal(size=nz)
         X = np.broadcast_to(x, (nz, ny, nx))
-        Y = np.broadcast_to(y, (nz, ny, nx))
-        Z = np.broadcast_to(z[:, None, None], (nz, ny, nx))
+        if gridtype == GRID2D_PLANE:
+            Y = np.broadcast_to(y, (nz, ny, nx))
+            Z = np.broadcast_to(z[:, None, None], (nz, ny, nx))
+        else:  # y holds R, z the angle: y = R cos(seta), z = R sin(seta)
+            Y = y[None] * np.cos(z)[:, None, None]
+            Z = y[None] * np.sin(z)[:, None, None]
     else:
         X, Y, Z = (rng.normal(size=(nz, ny, nx)) for _ in range(3))
         x, y, z = X, Y, Z
+        if gridtype == GRID_AND_JACOBIAN3D:
+            jac = [rng.normal(size=(nz, ny, nx)) for _ in range(10)]
+    return (x, y, z, jac), (X, Y, Z, jac)
+
+
+@pytest.mark.parametrize("gridtype", [GRID1D, GRID2D_PLANE, GRID2D_AXIAL_SYMM, GRID3D, GRID_AND_JACOBIAN3D])
+def test_grid_file_round_trip(tmp_path, gridtype):
+    nx, ny, nz = 6, 5, 4
+    (x, y, z, jac), (X, Y, Z, J) = _grid_case(gridtype, nx, ny, nz)
     path = str(tmp_path / "OCFD-grid.dat")
-    fileio.write_grid(path, gridtype, x, y, z)
+    fileio.write_grid(path, gridtype, x, y, z, jac=jac)
     got = fileio.read_grid(path, gridtype, nx, ny, nz)
-    for a, b in zip(got, (X, Y, Z)):
+    assert len(got) == (4 if gridtype == GRID_AND_JACOBIAN3D else 3)
+    for a, b in zip(got[:3], (X, Y, Z)):
         np.testing.assert_array_equal(a, b)
+    if J is not None:
+        for a, b in zip(got[3], J):
+            np.testing.assert_array_equal(a, b)
+    if gridtype == GRID_AND_JACOBIAN3D:
+        with pytest.raises(ValueError):
+            fileio.write_grid(path, gridtype, x, y, z)
+
+
+@pytest.mark.parametrize("gridtype", [GRID2D_AXIAL_SYMM, GRID_AND_JACOBIAN3D])
+def test_driver_reads_grid_files_like_python(driver, tmp_path, gridtype):
+    """The C++ host reads a grid file written by the Python host into the same
+    coordinates (bit for bit; the axisymmetric y and z within an ulp, since the
+    two evaluate cos and sin with different libraries) and metric arrays."""
+    nx, ny, nz = 7, 6, 5
+    (x, y, z, jac), _ = _grid_case(gridtype, nx, ny, nz)
+    path = str(tmp_path / "OCFD-grid.dat")
+    fileio.write_grid(path, gridtype, x, y, z, jac=jac)
+    out = str(tmp_path / "dump.bin")
+    subprocess.run([driver, "--grid-dump", str(gridtype), str(nx), str(ny), str(nz), path, out], check=True)
+    got = np.fromfile(out, dtype="<f8").reshape(-1, nz, ny, nx)
+    want = fileio.read_grid(path, gridtype, nx, ny, nz)
+    arrays = list(want[:3]) + (list(want[3]) if gridtype == GRID_AND_JACOBIAN3D else [])
+    assert got.shape[0] == len(arrays)
+    np.testing.assert_array_equal(got[0], arrays[0])
+    for a, b in zip(got[1:], arrays[1:]):
+        if gridtype == GRID2D_AXIAL_SYMM:
+            np.testing.assert_allclose(a, b, rtol=4.5e-16, atol=1e-300)
+        else:
+            np.testing.assert_array_equal(a, b)

@@ -81,7 +81,9 @@ enum {
                             (OCFD_handle_NegativeT.f90:13-16 / OCFD_Time_Adv.f90:118-121) */
   OCFD_E_STATE = -4,     /* call out of order (e.g. step before metrics) */
   OCFD_E_NOMEM = -5,
-  OCFD_E_TIMEOUT = -6    /* a bounded device wait gave up */
+  OCFD_E_TIMEOUT = -6    /* a bounded device wait gave up: the results of the steps since the
+                            last synchronisation are invalid (restart from a kept state); the
+                            handle stages its face tiles with plain loads from then on */
 };
 
 /*
@@ -183,6 +185,14 @@ int ocfd_gpu_upload_metrics(ocfd_handle* h, const double* const metrics[OCFD_N_M
  * means mesh_gen('box') (OCFD_mesh.f90:319-354). */
 int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const double* z);
 
+/* init_mesh for Iflag_Gridtype = GRID_AND_JACOBIAN3D (31): read_mesh3d reads
+ * the metrics and the Jacobian from the grid file with the coordinates
+ * (OCFD_mesh.f90:187-217) and init_mesh skips comput_Jacobian3d (:24-26); the
+ * rest is ocfd_gpu_init_mesh.  jac: ten interior (nx,ny,nz) arrays in Fortran
+ * order, Akx, Aky, Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Ajac. */
+int ocfd_gpu_init_mesh_jacobian(ocfd_handle* h, const double* x, const double* y, const double* z,
+                                const double* const jac[10]);
+
 /* Download the 22 haloed metric arrays (for checks and for the host's analysis). */
 int ocfd_gpu_download_metrics(ocfd_handle* h, double* const metrics[OCFD_N_METRICS]);
 
@@ -279,6 +289,11 @@ int ocfd_gpu_advance_clock(ocfd_handle* h);
  * status of every stage is checked on the device; a failure is reported by
  * the next synchronous call (and by this one when sync != 0). */
 int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync);
+/* Kernels launched by one captured time step of ocfd_gpu_step (the kernel
+ * nodes of its CUDA graph), or -1 before the first captured step or when the
+ * step runs without a graph (filtering, time-dependent wall data).  The
+ * reference has no counterpart (launch accounting of the device path). */
+int ocfd_gpu_step_kernels(const ocfd_handle* h);
 
 /* Run nsteps fused steps eagerly (no graph) with CUDA events around each kernel
  * group on the instance's stream; ms[] receives the average milliseconds per
@@ -333,12 +348,16 @@ int ocfd_gpu_download_block(ocfd_handle* h, int ib, int ie, int jb, int je, int 
  *   ajac   device haloed Jacobian, same layout
  *   stream cudaStream_t (NULL: the default stream); the call waits for it
  * E0 receives the same three averages as ocfd_gpu_show_flow_msg (equal within
- * rounding: the summation order differs).  The partial sums live in a fixed
- * static device array of OCFD_NOALLOC_MAX_PLANES k-planes: nz above that is
- * rejected with OCFD_E_PARAM.  Nothing in that array has to start at zero.
- * The first call on a device, made with that device current, looks up the
- * array's address (once per device); make that first call before any stream
- * capture begins.  There is one array per device, so overlapping calls on the
+ * rounding: the summation order differs).  Every call copies its three sums to
+ * host memory and waits for the stream before it returns.  The partial sums
+ * live in a fixed static device array of OCFD_NOALLOC_MAX_PLANES partial
+ * blocks: nz above OCFD_NOALLOC_MAX_PLANES is rejected with OCFD_E_PARAM.
+ * Nothing in that array has to start at zero.  The first call on a device,
+ * made with that device current, looks up the array's address (once per
+ * device) and keeps it for the life of the process; make that first call
+ * before any stream capture begins.  A cudaDeviceReset of that device makes
+ * the kept address stale: do not use this entry point on a device after
+ * resetting it.  There is one array per device, so overlapping calls on the
  * same device (from several streams or host threads) race: serialise them. */
 #define OCFD_NOALLOC_MAX_PLANES 4096
 int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f, const double* const prims[5],

@@ -54,10 +54,12 @@ struct ocfd_handle {
     double* fn;
     double* t;
     cudaGraphExec_t g;
+    int kernels;  // kernel nodes of the captured step
   } graphs[4] = {};
   int ngraphs = 0;
   bool halo_valid = false;
   bool metrics_ready = false;
+  bool tma_off = false;  // a bounded TMA wait gave up: face tiles are staged with plain loads
   int met_version = 0;  // bumped whenever the metrics (and Phys::metzero) change
   // BC_BoundaryLayer / BC_SweptCorner boundary data (device) and time factor (host)
   double* bl_inlet = nullptr;
@@ -298,7 +300,20 @@ int ocfd_gpu_sync(ocfd_handle* h) {
   CK(cudaStreamSynchronize(h->st));
   if (h->hstat->error == 3)
     return fail(h, OCFD_E_NEGT, "Number of Negative Temperature Points >  Limit, STOP !");
-  if (h->hstat->error == 4) return fail(h, OCFD_E_TIMEOUT, "a bounded device wait gave up (tile copy)");
+  if (h->hstat->error == 4) {
+    // The stage that timed out left invalid face fluxes; the caller restarts
+    // from a state it keeps.  Later launches of this handle stage face tiles
+    // with plain loads (the captured step graphs hold TMA launches: dropped).
+    h->tma_off = true;
+    for (int q = 0; q < h->ngraphs; q++)
+      if (h->graphs[q].g) cudaGraphExecDestroy(h->graphs[q].g);
+    h->ngraphs = 0;
+    CK(cudaMemsetAsync(&h->dstat->error, 0, sizeof(int), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return fail(h, OCFD_E_TIMEOUT,
+                "a bounded device wait gave up (tile copy): the results of the steps since the last "
+                "synchronisation are invalid; this handle no longer uses TMA tile staging");
+  }
   return OCFD_OK;
 }
 
@@ -473,12 +488,15 @@ int ocfd_gpu_upload_metrics(ocfd_handle* h, const double* const metrics[OCFD_N_M
   return OCFD_OK;
 }
 
-int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const double* z) {
+// init_mesh (OCFD_mesh.f90:1-58) from interior coordinates (NULL: mesh_gen('box'))
+// and, for GRID_AND_JACOBIAN3D, the interior metrics and Jacobian of the grid file.
+static int init_mesh_common(ocfd_handle* h, const double* x, const double* y, const double* z,
+                            const double* const jac[10]) {
   if (!h) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));
   const Grid& g = h->g;
+  double* tmp = h->scratch;  // nh >= n doubles
   if (x && y && z) {
-    double* tmp = h->scratch;  // nh >= n doubles
     const double* src[3] = {x, y, z};
     for (int q = 0; q < 3; q++) {
       CK(cudaMemcpyAsync(tmp, src[q], g.n * 8, cudaMemcpyHostToDevice, h->st));
@@ -487,14 +505,31 @@ int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const d
   } else {
     k_box<<<148 * 8, 256, 0, h->st>>>(g, h->met[0], h->met[1], h->met[2]);
   }
+  if (jac)
+    for (int m = 0; m < 10; m++) {
+      CK(cudaMemcpyAsync(tmp, jac[m], g.n * 8, cudaMemcpyHostToDevice, h->st));
+      k_scatter_interior<<<148 * 8, 256, 0, h->st>>>(g, tmp, h->met[OCFD_M_AKX + m]);
+    }
   CK(cudaGetLastError());
-  CK(launch_mesh(g, h->ph, h->dc, h->met, h->p.periodic_span, h->st));
+  CK(launch_mesh(g, h->ph, h->dc, h->met, h->p.periodic_span, jac != nullptr, h->st));
   int r = refresh_met32(h);
   if (r) return r;
   r = refresh_metzero(h);
   if (r) return r;
   h->metrics_ready = true;
   return OCFD_OK;
+}
+
+int ocfd_gpu_init_mesh(ocfd_handle* h, const double* x, const double* y, const double* z) {
+  return init_mesh_common(h, x, y, z, nullptr);
+}
+
+int ocfd_gpu_init_mesh_jacobian(ocfd_handle* h, const double* x, const double* y, const double* z,
+                                const double* const jac[10]) {
+  if (!x || !y || !z || !jac) return OCFD_E_PARAM;
+  for (int m = 0; m < 10; m++)
+    if (!jac[m]) return OCFD_E_PARAM;
+  return init_mesh_common(h, x, y, z, jac);
 }
 
 unsigned int ocfd_gpu_metric_zero_mask(const ocfd_handle* h) { return h ? h->ph.metzero : 0u; }
@@ -662,6 +697,7 @@ static FaceArgs<S> face_args(ocfd_handle* h, int d) {
   a.fend = g.len(d);
   a.split = h->p.flux_splitting;
   a.err = &h->dstat->error;
+  a.no_tma = h->tma_off ? 1 : 0;
   return a;
 }
 
@@ -1044,6 +1080,21 @@ extern "C" int ocfd_gpu_profile_steps(ocfd_handle* h, int nsteps, double ms[8]) 
   return OCFD_OK;
 }
 
+// Kernel nodes of a captured graph (-1 if the graph cannot be inspected).
+static int graph_kernel_nodes(cudaGraph_t graph) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return -1;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return -1;
+  int k = 0;
+  for (size_t q = 0; q < n; q++) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[q], &t) != cudaSuccess) return -1;
+    if (t == cudaGraphNodeTypeKernel) k++;
+  }
+  return k;
+}
+
 int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
   if (!h || nsteps < 0) return OCFD_E_PARAM;
   CK(cudaSetDevice(h->device));
@@ -1079,6 +1130,7 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
         if (r) return r;
         if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
         slot = &h->graphs[h->ngraphs];
+        slot->kernels = graph_kernel_nodes(graph);
         e = cudaGraphInstantiate(&slot->g, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
@@ -1103,6 +1155,11 @@ int ocfd_gpu_step(ocfd_handle* h, int nsteps, int sync) {
   return OCFD_OK;
 }
 
+int ocfd_gpu_step_kernels(const ocfd_handle* h) {
+  if (!h || h->ngraphs == 0) return -1;
+  return h->graphs[h->ngraphs - 1].kernels;
+}
+
 // ------------------------------------------------------------------ diagnostics
 int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]) {
   if (!h || !E0) return OCFD_E_PARAM;
@@ -1110,7 +1167,7 @@ int ocfd_gpu_show_flow_msg(ocfd_handle* h, double E0[3]) {
   CK(launch_flow_msg(h->g, h->ph, h->f, h->prim, h->met[OCFD_M_AJAC], h->scratch, h->dout, h->st));
   CK(cudaMemcpyAsync(h->hout, h->dout, 3 * 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  const double N = (double)(h->p.nx * h->p.ny * h->p.nz);
+  const double N = (double)h->g.n;
   for (int q = 0; q < 3; q++) E0[q] = h->hout[q] / N;
   return OCFD_OK;
 }
@@ -1201,7 +1258,7 @@ int ocfd_gpu_ana_box(ocfd_handle* h, double out[20]) {
   CK(launch_ana_box(h->g, h->ph, h->dc, h->prim, h->met, h->scratch, h->dout, h->dout + 16, h->st));
   CK(cudaMemcpyAsync(h->hout, h->dout, 17 * 8, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  const double N = (double)(h->p.nx * h->p.ny * h->p.nz);
+  const double N = (double)h->g.n;
   double a[14];
   for (int q = 0; q < 14; q++) a[q] = h->hout[q] / N;
   double u_rms = a[0], v_rms = a[1], w_rms = a[2], Ux_rms = a[3], Ux_sk = a[4], Ux_fl = a[5], d_aver = a[6];

@@ -197,6 +197,7 @@ struct FaceArgs {
   int fbeg, fend;    // faces computed: fbeg..fend
   int split;         // 1 SW, 2 LLF
   int* err;          // DevStatus::error of the instance (bounded waits record 4 there)
+  int no_tma;        // host side: stage the tile with plain loads (a TMA wait of this instance gave up)
   Phys ph;
 };
 

@@ -1078,6 +1078,9 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
   const int c0 = x0 - toff;
   const int c1 = DIR == 0 ? pbase + 4 : (DIR == 1 ? g0 : bz + 4);
   const int c2 = DIR == 2 ? g0 : bz + 4;
+  // once a block of this instance has given up on its tile copies (error 4),
+  // the launch's results are invalid: later blocks issue no copies and leave
+  if (__syncthreads_or(threadIdx.x == 0 && *reinterpret_cast<volatile const int*>(a.err) == 4)) return;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
@@ -1201,7 +1204,7 @@ cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cud
   // TMA staging for the FP64 sweeps (measured 1-3% faster at 256^3); the FP32
   // sweeps, four blocks per SM, are as fast or faster with plain loads
   if constexpr (sizeof(S) == 8)
-  if (allin && (a.g.n == 0 || (face_tma_enabled() && tma_strides_ok<S>(a.g)))) {
+  if (allin && (a.g.n == 0 || (!a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g)))) {
     // set-up (empty grid) registers both kernels; launches take the TMA path
 #define OCFD_FACE_TMA_CASE(D, C, SC)                                                        \
     if (dir == D && chr == C && scheme == SC) {                                               \

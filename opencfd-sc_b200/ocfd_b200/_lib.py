@@ -72,6 +72,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_gpu_download_metrics.restype = C.c_int
     L.ocfd_gpu_init_mesh.argtypes = [H, dp, dp, dp]
     L.ocfd_gpu_init_mesh.restype = C.c_int
+    L.ocfd_gpu_init_mesh_jacobian.argtypes = [H, dp, dp, dp, dp * 10]
+    L.ocfd_gpu_init_mesh_jacobian.restype = C.c_int
     L.ocfd_gpu_upload_state.argtypes = [H, dp, C.c_void_p, C.c_int, C.c_double]
     L.ocfd_gpu_upload_state.restype = C.c_int
     L.ocfd_gpu_init3d.argtypes = [H, dp * 5, C.c_int, C.c_double]
@@ -90,6 +92,8 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_gpu_duvwt.restype = C.c_int
     L.ocfd_gpu_step.argtypes = [H, C.c_int, C.c_int]
     L.ocfd_gpu_step.restype = C.c_int
+    L.ocfd_gpu_step_kernels.argtypes = [H]
+    L.ocfd_gpu_step_kernels.restype = C.c_int
     L.ocfd_gpu_show_flow_msg.argtypes = [H, dp]
     L.ocfd_gpu_show_flow_msg.restype = C.c_int
     L.ocfd_gpu_ana_box.argtypes = [H, dp]
@@ -152,5 +156,6 @@ EXPORTED = [
     "ocfd_batch_step", "ocfd_batch_destroy", "ocfd_gpu_profile_steps", "ocfd_show_flow_msg_noalloc",
     "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error", "ocfd_gpu_metric_zero_mask",
     "ocfd_gpu_set_bc_layer", "ocfd_gpu_ana_q", "ocfd_gpu_ana_time_average", "ocfd_gpu_download_average",
-    "ocfd_gpu_upload_average", "ocfd_gpu_ana_corner", "ocfd_gpu_download_block",
+    "ocfd_gpu_upload_average", "ocfd_gpu_ana_corner", "ocfd_gpu_download_block", "ocfd_gpu_step_kernels",
+    "ocfd_gpu_init_mesh_jacobian",
 ]

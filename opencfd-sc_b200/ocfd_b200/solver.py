@@ -83,13 +83,21 @@ class Solver:
         self._check(self.L.ocfd_gpu_sync(self.h), "sync")
 
     # ------------------------------------------------------------------ init (init3d)
-    def init_mesh(self, x=None, y=None, z=None):
-        """init_mesh (OCFD_mesh.f90:1-58) on the device; None -> mesh_gen('box')."""
+    def init_mesh(self, x=None, y=None, z=None, jac=None):
+        """init_mesh (OCFD_mesh.f90:1-58) on the device; None -> mesh_gen('box').
+        jac: the ten interior metric arrays Akx..Asz, Ajac of a GRID_AND_JACOBIAN3D
+        grid file (comput_Jacobian3d is then skipped)."""
         if x is None:
             self._check(self.L.ocfd_gpu_init_mesh(self.h, None, None, None), "init_mesh")
-        else:
-            xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+            return
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        if jac is None:
             self._check(self.L.ocfd_gpu_init_mesh(self.h, _dp(xs[0]), _dp(xs[1]), _dp(xs[2])), "init_mesh")
+        else:
+            js = [np.ascontiguousarray(a, dtype=np.float64) for a in jac]
+            arr = (C.POINTER(C.c_double) * 10)(*[_dp(a) for a in js])
+            self._check(self.L.ocfd_gpu_init_mesh_jacobian(self.h, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]), arr),
+                        "init_mesh")
 
     def upload_metrics(self, metrics):
         ms = [np.ascontiguousarray(m, dtype=np.float64) for m in metrics]
@@ -218,6 +226,10 @@ class Solver:
     def step(self, n: int = 1, sync: bool = True):
         """n time steps on the fused, graph-captured path."""
         self._check(self.L.ocfd_gpu_step(self.h, n, 1 if sync else 0), "step")
+
+    def step_kernels(self) -> int:
+        """Kernels one captured time step launches (-1 before the first captured step)."""
+        return int(self.L.ocfd_gpu_step_kernels(self.h))
 
     PROFILE_GROUPS = ["sensor", "face_x", "face_y", "face_z", "visc_grad", "stage_tail", "negt_bc_halo", "step"]
 

@@ -14,13 +14,22 @@ reference's negative-temperature error after 17 steps at that CFL, and after 21
 steps at dt = 0.001 for the characteristic OMP6 path); dt = 0.0005 (CFL 0.22)
 is used.  The metric does not depend on dt.
 
+The metric compares FP64 with mixed precision at a stated error: an FP64 line
+(the default) carries a "mixed" object timed the same way -- FP32 flux
+splitting, characteristic projection, reconstruction and viscous derivatives,
+FP64 state, metrics, primitive recovery and RK3 combination -- with its speed
+over FP64 and its errors against the FP64 run (kinetic energy and enstrophy
+histories, relative L2 / Linf of rho, u and p) after the workload's stated
+number of steps, both runs from the same initial field.
+
 Multi-GPU: the path does not shard in this build (one grid per GPU); N GPUs run
 N independent replicas ("replicas only", weak scaling), the time is the max
 over ranks and the value is the total grid-point updates of all ranks.
 
 --impl reference times the CPU restatement of the reference (the oracle, all
-host threads via OpenMP) on the same configuration; each of its steps is one
-time step of a 128^3 sample of the workload (1/8 of the points).
+host threads via OpenMP) on the same configuration: each of its steps is one
+full time step of the workload's own grid (the 512^3 isotropic turbulence,
+about 80 GB on the host, is sampled on 128^3).
 """
 from __future__ import annotations
 
@@ -100,12 +109,10 @@ def make_params(workload: str, precision: str, n_override: int | None = None):
     n, scheme, chr_, split, dt, _ = WORKLOADS[workload]
     if n_override:
         n = n_override
-    p = cases.tgv_params(n, scheme=SCHEME[scheme], character=chr_, split=split, dt=dt)
-    if scheme == "HYBRID":
-        p.hybrid_para[0] = 1
-        p.hybrid_para[1] = 0.004
-        p.hybrid_para[2] = 0.01
-        p.ud7l_diss = 0.0
+    if chr_ == 1:
+        p = cases.tgv_char_params(n, scheme, dt=dt)
+    else:
+        p = cases.tgv_params(n, scheme=SCHEME[scheme], character=chr_, split=split, dt=dt)
     p.precision = 1 if precision == "mixed" else 0
     return p
 
@@ -239,35 +246,25 @@ def data_kind(workload: str) -> str:
     return "synthetic (seeded isotropic-turbulence field)"
 
 
-def cpu_sample(workload: str, steps: int, warm: int):
-    """The oracle on a bounded sample of `workload`: (rate, seconds, sample name,
-    sample params, workload description, workload points per step)."""
+def cpu_case(workload: str):
+    """(params, coordinates or None, interior primitives, sample description) of
+    the oracle's CPU run: the workload itself, except for the 512^3 isotropic
+    turbulence (about 80 GB of host memory and a minute per step on the oracle),
+    which is sampled on 128^3 with the same set-up."""
     from ocfd_b200 import cases
 
-    if workload in WORKLOADS:
-        wl = WORKLOADS[workload]
-        desc, npts = wl[5], wl[0] ** 3
-        nsample = min(wl[0], 128)
-        p = make_params(workload, "fp64", n_override=nsample)
-        rate, secs = cpu_rate(p, steps, warm=warm)
-        what = f"TGV {nsample}^3"
-    elif workload == "cylinder_weno7_char":
-        desc = CASE_WORKLOADS[workload]
-        p = cases.cylinder_params()
-        npts = p.nx * p.ny * p.nz
-        rate, secs = cpu_rate(p, steps, warm=warm, xyz=cases.cylinder_grid(p.nx, p.ny, p.nz),
-                              prims=cases.cylinder_prims(p.nx, p.ny, p.nz))
-        what = "the cylinder case"
-    else:  # isotropic turbulence: a 128^3 sample of the same set-up
-        desc, npts = CASE_WORKLOADS[workload], 512 ** 3
+    if workload == "hit512_hybrid_llf":
         p = cases.hit_params(128, re=1000.0, ma=1.0, dt=1e-3)
-        rate, secs = cpu_rate(p, steps, warm=warm, xyz=cases.hit_coords(128),
-                              prims=cases.hit_prims(128, mt=0.6, ma=1.0))
-        what = "isotropic turbulence 128^3"
-    return rate, secs, what, p, desc, npts
+        return (p, cases.hit_coords(128), cases.hit_prims(128, mt=0.6, ma=1.0),
+                "isotropic turbulence 128^3 with the same scheme (1/64 of the workload's points per step)")
+    p, xyz, prims = make_case(workload, "fp64")
+    return p, xyz, prims, f"the {grid_name(p)} workload itself (same scheme and grid)"
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference (oracle, all host
+    threads) on the workload's own grid -- every step is one full time step of
+    the same configuration as the GPU arm."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -275,17 +272,18 @@ def run_reference(args):
 
     cores = multiprocessing.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    rate, secs, what, p, desc, npts = cpu_sample(args.workload, args.steps, args.warmup)
-    nsample_pts = p.nx * p.ny * p.nz
-    ms = secs / args.steps * 1e3 * npts / nsample_pts
-    sample = (f"{args.steps} time steps of {what} (same scheme; {nsample_pts} of the workload's "
-              f"{npts} points per step) after {args.warmup} warm-up steps")
-    grid = f"{p.nx}x{p.ny}x{p.nz}"
+    p, xyz, prims, what = cpu_case(args.workload)
+    rate, secs = cpu_rate(p, args.steps, warm=args.warmup, xyz=xyz, prims=prims)
+    del prims, xyz
+    ms = secs / args.steps * 1e3
+    desc = WORKLOADS[args.workload][5] if args.workload in WORKLOADS else CASE_WORKLOADS[args.workload]
+    sample = f"{args.steps} time steps of {what}, {p.nx * p.ny * p.nz} points a step, after {args.warmup} warm-up steps"
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": data_kind(args.workload),
-        "config": {"workload": args.workload, "description": desc, "sample_grid": grid},
+        "config": {"workload": args.workload, "description": desc, "grid": grid_name(p), "dt": p.dt,
+                   "precision": "fp64"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -294,7 +292,162 @@ def run_reference(args):
     return 0
 
 
+def grid_name(p) -> str:
+    return f"{p.nx}^3" if p.nx == p.ny == p.nz else f"{p.nx}x{p.ny}x{p.nz}"
+
+
+# steps of the stated run of each workload: the horizon of the mixed-vs-FP64 errors
+HORIZON = {"tgv256_omp6_char": 500, "tgv256_hybrid_char": 500, "tgv256_weno7": 500, "tgv64_weno7": 100,
+           "hit512_hybrid_llf": 300, "cylinder_weno7_char": 2000}
+
+
 # ---------------------------------------------------------------------------------------------
+def _timed(s, steps: int, warmup: int, local: int, dist: bool):
+    """W untimed steps, then K steps between CUDA events on the solver's stream
+    (max over ranks), with the clocks sampled during the timed region."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(s.stream, device=local)
+    s.step(warmup, sync=True)  # includes graph capture
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.step(steps, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        import torch.distributed as tdist
+
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    s.sync()  # raises if the run hit the reference's negative-temperature stop
+    return ms, clk.summary()
+
+
+def _kernels(s, n: int, peak: float, workload: str, precision: str):
+    """Per-kernel CUDA-event split of 3 eager steps and the roofline of the dominant kernel."""
+    prof = s.profile_steps(3)
+    model = byte_model(s.p, s.metric_zero_mask())
+    groups = {k: v for k, v in prof.items() if k in model}
+    dom = max(groups, key=groups.get)
+    t_launch = groups[dom] / 3.0 * 1e-3  # 3 launches per step
+    achieved = model[dom] * n / t_launch / 1e9
+    bpp = load_traffic().get(f"{workload}:{precision}:{dom}")
+    return {"kernel": dom, "achieved": achieved, "frac": achieved / peak, "bytes_per_point": model[dom],
+            "traffic": None if bpp is None else bpp * n,
+            "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+            "hbm_frac_by_kernel": {k: round(model[k] * n / (groups[k] / 3.0 * 1e-3) / 1e9 / peak, 3)
+                                   for k in groups if groups[k] > 0}}
+
+
+def _e2e(s, steps: int, dist: bool, local: int):
+    """Same metric end to end through the C ABI with a host-owned state.  Headline
+    mode: the host owns the conserved variables f (the reference's time-loop
+    state); per step f is uploaded from pinned host memory, the primitives are
+    derived from it on the device (comput_duvwT), one time step runs and f is
+    downloaded.  Second mode: f and the haloed primitives both ways."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    f_host = torch.empty(s.shape5, dtype=torch.float64, pin_memory=True).numpy()
+    prim_host = [torch.empty(s.shape_h, dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
+    L = s.L
+    dp = C.POINTER(C.c_double)
+    fptr = f_host.ctypes.data_as(dp)
+    parr = (dp * 5)(*[a.ctypes.data_as(dp) for a in prim_host])
+    L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
+    istep, tt = s.time()
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+    nneg = C.c_int(0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        L.ocfd_gpu_upload_state(s.h, fptr, None, istep, tt)
+        L.ocfd_gpu_duvwt(s.h, C.byref(nneg))
+        L.ocfd_gpu_step(s.h, 1, 0)
+        L.ocfd_gpu_download_state(s.h, fptr, None)
+        istep, tt = s.time()
+    t_e2e = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        L.ocfd_gpu_upload_state(s.h, fptr, C.cast(parr, C.c_void_p), istep, tt)
+        L.ocfd_gpu_step(s.h, 1, 0)
+        L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
+        istep, tt = s.time()
+    t_full = time.perf_counter() - t0
+    if dist:
+        import torch.distributed as tdist
+
+        t = torch.tensor([t_e2e, t_full], device=f"cuda:{local}", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        t_e2e, t_full = float(t[0].item()), float(t[1].item())
+    s.sync()
+    n = s.nx * s.ny * s.nz
+    return t_e2e, t_full, 5 * 8 * n, 5 * 8 * (n + int(np.prod(s.shape_h)))
+
+
+def _history(s, prims, steps: int, every: int):
+    """Restart from the initial field and run `steps` steps: kinetic energy
+    (show_flow_msg) and enstrophy (ana_box) every `every` steps, and the final
+    interior rho, u, v, w, p."""
+    import numpy as np
+
+    s.init3d(prims)
+    ke, ens = [float(s.show_flow_msg()[1])], [float(s.ana_box()[13])]
+    done = 0
+    while done < steps:
+        k = min(every, steps - done)
+        s.step(k)
+        done += k
+        ke.append(float(s.show_flow_msg()[1]))
+        ens.append(float(s.ana_box()[13]))
+    _, pr = s.download_state()
+    inner = (slice(4, -4),) * 3
+    d, u, v, w, T = [np.ascontiguousarray(a[inner]) for a in pr]
+    p = d * T / (s.p.gamma * s.p.ma * s.p.ma)  # p = rho T / (gamma Ma^2)
+    return {"ke": np.array(ke), "enstrophy": np.array(ens), "rho": d, "vel": (u, v, w), "p": p}
+
+
+def _errors(a: dict, b: dict) -> dict:
+    """Errors of run a against run b (relative L2 and Linf on the interior)."""
+    import numpy as np
+
+    def rel(x, y):
+        return abs(x - y) / abs(y)
+
+    def l2(x, y):
+        return float(np.sqrt(np.sum((x - y) ** 2) / np.sum(y ** 2)))
+
+    def linf(x, y):
+        return float(np.max(np.abs(x - y)) / np.max(np.abs(y)))
+
+    du2 = sum(np.sum((x - y) ** 2) for x, y in zip(a["vel"], b["vel"]))
+    u2 = sum(np.sum(y ** 2) for y in b["vel"])
+    dumax = max(float(np.max(np.abs(x - y))) for x, y in zip(a["vel"], b["vel"]))
+    umax = max(float(np.max(np.abs(y))) for y in b["vel"])
+    return {"ke_rel": float(rel(a["ke"][-1], b["ke"][-1])),
+            "ke_rel_max_history": float(np.max(np.abs(a["ke"] - b["ke"]) / np.abs(b["ke"]))),
+            "enstrophy_rel": float(rel(a["enstrophy"][-1], b["enstrophy"][-1])),
+            "enstrophy_rel_max_history": float(np.max(np.abs(a["enstrophy"] - b["enstrophy"]) /
+                                                      np.abs(b["enstrophy"]))),
+            "rho": {"l2_rel": l2(a["rho"], b["rho"]), "linf_rel": linf(a["rho"], b["rho"])},
+            "u": {"l2_rel": float(np.sqrt(du2 / u2)), "linf_rel": dumax / umax},
+            "p": {"l2_rel": l2(a["p"], b["p"]), "linf_rel": linf(a["p"], b["p"])}}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -312,102 +465,65 @@ def run_ours(args):
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
 
-    from ocfd_b200 import cases
-    from ocfd_b200.solver import Solver
+    from ocfd_b200.solver import Solver, footprint
 
     p, xyz, prims = make_case(args.workload, args.precision)
     n = p.nx * p.ny * p.nz
-    s = Solver(p, device=local)
-    if xyz is None:
-        s.init_mesh()
-    else:
-        s.init_mesh(*xyz)
-    s.init3d(prims)
-    del prims, xyz
-    stream = torch.cuda.ExternalStream(s.stream, device=local)
-
-    s.step(args.warmup, sync=True)  # includes graph capture
-    if dist:
-        tdist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        s.step(args.steps, sync=False)
-        e1.record(stream)
-        e1.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
-    s.sync()
-    value = world * n * args.steps / (ms * 1e-3) / 1e9
-    clocks = clk.summary()
-
-    # kernels launched per step on the fused path
-    per_stage = 3 + (1 if p.if_viscous else 0) + 2
-    launches = args.steps * (3 * per_stage + (1 if p.scheme_invis == 10 else 0))
-
-    # ---- per-kernel timing (roofline of the dominant kernel)
-    prof = s.profile_steps(3)
-    model = byte_model(s.p, s.metric_zero_mask())
-    groups = {k: v for k, v in prof.items() if k in model}
-    dom = max(groups, key=groups.get)
-    t_launch = groups[dom] / 3.0 * 1e-3  # 3 launches per step
-    achieved = model[dom] * n / t_launch / 1e9
     peak, peak_kind = load_peaks()
-    bpp = load_traffic().get(f"{args.workload}:{args.precision}:{dom}")
-    traffic = None if bpp is None else bpp * n  # DRAM bytes per launch, scaled from a 128^3 capture
+    horizon = args.err_steps if args.err_steps is not None else HORIZON[args.workload]
+    every = max(1, horizon // 10)
 
-    # ---- end to end through the C ABI with host-owned state.  Headline mode: the
-    # host owns the conserved variables f (the reference's time-loop state); per
-    # step f is uploaded from pinned host memory, the primitives are derived from
-    # it on the device (comput_duvwT), one time step runs and f is downloaded.
-    # Second mode: f and the haloed primitives both ways.
+    def start(q):
+        s = Solver(q, device=local)
+        if xyz is None:
+            s.init_mesh()
+        else:
+            s.init_mesh(*xyz)
+        s.init3d(prims)
+        return s
+
+    # ---- the line's own precision: timed steps, kernel split, end to end
+    s = start(p)
+    ms, clocks = _timed(s, args.steps, args.warmup, local, dist)
+    value = world * n * args.steps / (ms * 1e-3) / 1e9
+    launches = args.steps * s.step_kernels()
+    kern = _kernels(s, n, peak, args.workload, args.precision)
     K2 = max(1, min(args.steps, 5))
-    f_host = torch.empty(s.shape5, dtype=torch.float64, pin_memory=True).numpy()
-    prim_host = [torch.empty(s.shape_h, dtype=torch.float64, pin_memory=True).numpy() for _ in range(5)]
-    import ctypes as C
-
-    L = s.L
-    dp = C.POINTER(C.c_double)
-    fptr = f_host.ctypes.data_as(dp)
-    parr = (dp * 5)(*[a.ctypes.data_as(dp) for a in prim_host])
-    L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
-    istep, tt = s.time()
-    if dist:
-        tdist.barrier()
-    nneg = C.c_int(0)
-    t0 = time.perf_counter()
-    for _ in range(K2):
-        L.ocfd_gpu_upload_state(s.h, fptr, None, istep, tt)
-        L.ocfd_gpu_duvwt(s.h, C.byref(nneg))
-        L.ocfd_gpu_step(s.h, 1, 0)
-        L.ocfd_gpu_download_state(s.h, fptr, None)
-        istep, tt = s.time()
-    t_e2e = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    for _ in range(K2):
-        L.ocfd_gpu_upload_state(s.h, fptr, C.cast(parr, C.c_void_p), istep, tt)
-        L.ocfd_gpu_step(s.h, 1, 0)
-        L.ocfd_gpu_download_state(s.h, fptr, C.cast(parr, C.c_void_p))
-        istep, tt = s.time()
-    t_full = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([t_e2e, t_full], device=f"cuda:{local}", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        t_e2e, t_full = float(t[0].item()), float(t[1].item())
+    t_e2e, t_full, bytes_f, bytes_state = _e2e(s, K2, dist, local)
     e2e = world * n * K2 / t_e2e / 1e9
     e2e_full = world * n * K2 / t_full / 1e9
-    bytes_f = 5 * 8 * n
-    bytes_state = 5 * 8 * (n + int(np.prod(s.shape_h)))
-    s.sync()  # raises if the run hit the reference's negative-temperature stop
     ke = s.show_flow_msg()[1]
     if not np.isfinite(ke):
         raise RuntimeError("non-finite kinetic energy: the run is invalid")
+    fp_bytes = footprint(s.p)
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        # ---- FP64 reference run over the error horizon, then the mixed-precision leg
+        ref = _history(s, prims, horizon, every)
+        s.close()
+        pm = p.copy()
+        pm.precision = 1
+        sm = start(pm)
+        ms_m, clocks_m = _timed(sm, args.steps, args.warmup, local, dist)
+        value_m = world * n * args.steps / (ms_m * 1e-3) / 1e9
+        launches_m = args.steps * sm.step_kernels()
+        kern_m = _kernels(sm, n, peak, args.workload, "mixed")
+        te_m, _, _, _ = _e2e(sm, K2, dist, local)
+        hm = _history(sm, prims, horizon, every)
+        sm.close()
+        err = _errors(hm, ref)
+        err["steps"] = horizon
+        err["against"] = "the FP64 run of this line, same initial field and steps"
+        mixed = {"value": value_m, "unit": UNIT, "ms_per_step": ms_m / args.steps, "mixed_over_fp64": value_m / value,
+                 "dtype": "f32 flux/reconstruction/viscous, f64 state/metrics/primitive recovery",
+                 "clocks": clocks_m, "gpu_launches": launches_m,
+                 "e2e": {"value": world * n * K2 / te_m / 1e9, "unit": UNIT, "h2d_bytes_per_step": bytes_f,
+                         "d2h_bytes_per_step": bytes_f},
+                 "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", **kern_m},
+                 "error_vs_fp64": err}
+    else:
+        s.close()
+    del prims, xyz
 
     line = None
     if rank == 0:
@@ -417,22 +533,26 @@ def run_ours(args):
 
             cores = multiprocessing.cpu_count()
             os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-            # about 10 s of the host's cores: 2 warm-up steps, then enough steps
-            rate, secs, what, _, _, _ = cpu_sample(args.workload, 2, 1)
-            nst = int(min(40, max(3, 10.0 / max(secs / 2, 1e-3))))
-            rate, secs, what, _, _, _ = cpu_sample(args.workload, nst, 1)
+            # about 10-30 s of the host's cores on the workload's own grid: 1 warm-up step,
+            # then enough full steps for about 10 s
+            q, qxyz, qprims, what = cpu_case(args.workload)
+            rate, secs = cpu_rate(q, 1, warm=1, xyz=qxyz, prims=qprims)
+            nst = int(min(40, max(2, 10.0 / max(secs, 1e-3))))
+            rate, secs = cpu_rate(q, nst, warm=1, xyz=qxyz, prims=qprims)
+            del qprims, qxyz
             cpu = {"value": rate, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                   "sample": f"{nst} time steps of {what} with the same scheme on the oracle ({secs:.1f} s)"}
+                   "sample": f"{nst} time steps of {what} on the oracle after 1 warm-up step ({secs:.1f} s)"}
         desc = WORKLOADS[args.workload][5] if args.workload in WORKLOADS else CASE_WORKLOADS[args.workload]
-        grid = f"{p.nx}^3" if p.nx == p.ny == p.nz else f"{p.nx}x{p.ny}x{p.nz}"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state",
             "data": data_kind(args.workload),
-            "config": {"workload": args.workload, "description": desc, "grid": grid, "dt": p.dt,
+            "config": {"workload": args.workload, "description": desc, "grid": grid_name(p), "dt": p.dt,
                        "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (the state is GBs)"},
+                       "l2": (f"device state {fp_bytes / 2**20:.0f} MiB (conserved and primitive fields, "
+                              f"metrics, face and viscous fluxes), all read every step: larger than the "
+                              f"126 MB L2, no flush")},
             "clocks": clocks,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_f, "d2h_bytes_per_step": bytes_f,
                     "mode": "host-owned conserved state f: upload f, primitives derived on the device "
@@ -441,21 +561,13 @@ def run_ours(args):
                                         "d2h_bytes_per_step": bytes_state,
                                         "mode": "upload f + haloed primitives, one step, download both"}},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_kind": peak_kind, "bytes_per_point": model[dom],
-                         "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
-                         # algorithmic bytes / measured HBM bandwidth, every kernel of the step
-                         "hbm_frac_by_kernel": {k: round(model[k] * n / (groups[k] / 3.0 * 1e-3) / 1e9 / peak, 3)
-                                                for k in groups if groups[k] > 0},
-                         "note": ("the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM "
-                                  "bound: ncu pipe and DRAM fractions per kernel in "
-                                  "profiles/kernels_tgv192_omp6_char.md")},
+            "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, **kern,
+                         "note": "the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM bound"},
+            "mixed": mixed,
             "cpu_baseline": cpu,
             "kinetic_energy": ke,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if dist:
         tdist.barrier()
         tdist.destroy_process_group()
@@ -586,6 +698,9 @@ def main():
     ap.add_argument("--workload", default="tgv256_omp6_char", choices=list(WORKLOADS) + list(CASE_WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of an FP64 line")
+    ap.add_argument("--err-steps", type=int, default=None,
+                    help="horizon of the mixed-vs-FP64 errors (default: the workload's stated step count)")
     ap.add_argument("--serve", action="store_true", help="served request stream instead of the step benchmark")
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")

@@ -54,6 +54,22 @@ def tgv_params(n: int, scheme=SCHEME_WENO7, character=0, ma=0.1, re=1600.0, dt=0
     return p
 
 
+def tgv_char_params(n: int, scheme: str, dt: float = 0.0005, steps: int = 500) -> OcfdParams:
+    """Characteristic-flux Taylor-Green decks of the 256^3 runs (du_inviscous_Character,
+    SW, CD6): "OMP6", or "HYBRID" with sensor 1, thresholds 0.004 / 0.01 and UD7L_Diss = 0
+    (the linear faces are CD8 central).  dt = 0.0005: the stated 0.002 is above the
+    stability limit of RK3 with these schemes at Ma 0.1 on 256^3."""
+    from .params import SCHEME
+
+    p = tgv_params(n, scheme=SCHEME[scheme], character=1, split=SPLIT_SW, dt=dt, steps=steps)
+    if scheme == "HYBRID":
+        p.hybrid_para[0] = 1
+        p.hybrid_para[1] = 0.004
+        p.hybrid_para[2] = 0.01
+        p.ud7l_diss = 0.0
+    return p
+
+
 def tgv_prims(p: OcfdParams):
     """TGV initial primitives: rho=1, u=sin x cos y cos z, v=-cos x sin y cos z, w=0,
     p = p0 + (cos2x+cos2y)(cos2z+2)/16, T = p/(rho p0), p0 = 1/(gamma Ma^2)."""

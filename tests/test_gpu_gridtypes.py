@@ -4,11 +4,12 @@ OCFD_mesh.f90:286-317) and the 3-D grid with its metrics and Jacobian in the
 file (Iflag_Gridtype 31, read_mesh3d with comput_Jacobian3d skipped,
 OCFD_mesh.f90:11,24-26,187-217).  Strict build: the 22 metric arrays and the
 state after three time steps are bit-identical to the oracle; production
-build: metrics within 1e-13, state within 1e-12 relative L2."""
+build: metrics within 1e-13 of the largest component of their row, state
+within 1e-12 relative L2."""
 import numpy as np
 import pytest
 
-from ocfd_testlib import annulus_case, curvilinear_case, interior, rel_err, rel_l2
+from ocfd_testlib import annulus_case, curvilinear_case, interior, rel_l2
 from ocfd_b200 import fileio
 from ocfd_b200.params import GRID2D_AXIAL_SYMM, GRID_AND_JACOBIAN3D
 from ocfd_b200.solver import Solver
@@ -27,14 +28,22 @@ def _run(p, mesh, prims, strict):
     return o, s
 
 
+# metric arrays compared on a common scale: the three components of a row
+# (an analytically zero component holds rounding noise only)
+GROUPS = [(0,), (1,), (2,), (3, 4, 5), (6, 7, 8), (9, 10, 11), (12,), (13, 14, 15), (16, 17, 18), (19, 20, 21)]
+
+
 def _check_pair(o, s, strict):
     mg = s.download_metrics()
-    for m in range(22):
-        a, b = interior(mg[m]), interior(o.metric(m))
-        if strict:
-            np.testing.assert_array_equal(a, b, err_msg=f"metric {m}")
-        else:
-            assert rel_err(a, b) <= 1e-13, (m, rel_err(a, b))
+    for grp in GROUPS:
+        scale = max(float(np.max(np.abs(interior(o.metric(m))))) for m in grp)
+        for m in grp:
+            a, b = interior(mg[m]), interior(o.metric(m))
+            if strict:
+                np.testing.assert_array_equal(a, b, err_msg=f"metric {m}")
+            else:
+                err = float(np.max(np.abs(a - b))) / scale
+                assert err <= 1e-13, (m, err)
     o.step(3)
     s.step(3)
     f = s.download_f()

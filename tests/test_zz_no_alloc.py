@@ -58,7 +58,7 @@ def _case(n, ny, nz):
     return params, ref, f, prims, ajac, torch.cuda.current_stream(dev).cuda_stream
 
 
-@pytest.mark.parametrize("shape", [(32, 24, 20), (64, 64, 4)], ids=["box", "thin"])
+@pytest.mark.parametrize("shape", [(32, 24, 20), (64, 64, 8)], ids=["box", "thin"])
 def test_noalloc_show_flow_msg_matches_handle_entry_point(shape):
     import torch
 

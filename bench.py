@@ -127,7 +127,8 @@ def byte_model(p, zero_mask: int = 0) -> dict:
     nz = lambda ms: sum(1 for m in ms if not (zero_mask >> m) & 1)
     nface = 5  # characteristic form: projected fluxes; flux-vector form: h(F+) + h(F-) per face
     face = {d: 5 * s + nz(range(13 + 3 * i, 16 + 3 * i)) * s + nface * r for i, d in enumerate(("x", "y", "z"))}
-    visc = 4 * s + nz(range(3, 22)) * s + 12 * r  # u,v,w,T + non-zero metrics in; 12 Ev out
+    # u,v,w,T + the non-zero metrics Akx..Asz and Akx1..Asz1 in (not Ajac); 12 Ev out
+    visc = 4 * s + nz(list(range(3, 12)) + list(range(13, 22))) * s + 12 * r
     # tail: 3 directions of faces + 12 Ev + Ajac + fn + f (2 of 3 stages) in; f + prims out.
     # Mixed precision on an all-periodic grid (BC_None, fused): stages 1-2 write only T of
     # the FP64 primitives; FP32 copies of d and u,v,w,T (20 bytes) every stage.

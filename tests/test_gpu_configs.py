@@ -6,6 +6,12 @@ production build within 1e-10 relative L2 (the stated FP64 bar); the
 kinetic-energy history (show_flow_msg every 10 steps) agrees to 1e-12.
 Mixed precision on the characteristic OMP6 TGV: relative kinetic-energy error
 below 1e-5 against the FP64 run (the stated mixed-precision bar).
+
+Config 4 at its stated size -- the Mach 6 cylinder, 301 x 401 x 8 body-fitted
+grid, characteristic WENO7, isothermal wall -- 10 steps against the oracle:
+strict build bit-identical, production build within 1e-10 relative L2.
+Config 3's set-up on 128^3 (isotropic turbulence, hybrid sensor 1, LLF,
+flux-vector form, dt at CFL 0.5) -- 5 steps against the oracle, the same bars.
 """
 import os
 
@@ -75,3 +81,43 @@ def test_mixed_precision_kinetic_energy_error():
     ke_err = abs(out[1][0] - out[0][0]) / out[0][0]
     assert ke_err < 1e-5, ke_err
     assert rel_l2(out[1][1], out[0][1]) < 1e-5
+
+
+def _run_pair(p, mesh, prims, steps):
+    """The oracle's state after `steps` steps, then the two builds'."""
+    o = Oracle(p)
+    o.init_mesh(*mesh)
+    o.init3d(prims)
+    o.step(steps)
+    ref = o.f.copy()
+    o.close()
+    out = {}
+    for strict in (True, False):
+        s = Solver(p, strict=strict)
+        s.init_mesh(*mesh)
+        s.init3d(prims)
+        s.step(steps)
+        out[strict] = s.download_f()
+        s.close()
+    return ref, out
+
+
+def test_config4_cylinder_full_size_10_steps():
+    p = cases.cylinder_params()
+    ref, out = _run_pair(p, cases.cylinder_grid(p.nx, p.ny, p.nz), cases.cylinder_prims(p.nx, p.ny, p.nz), 10)
+    np.testing.assert_array_equal(out[True], ref)
+    err = rel_l2(out[False], ref)
+    assert err < 1e-10, err
+
+
+def test_config3_isotropic_turbulence_128_5_steps():
+    import math
+
+    n, ma = 128, 1.0
+    prims = cases.hit_prims(n, mt=0.6, ma=ma)
+    vmax = float(np.max(np.abs(prims[1]) + np.abs(prims[2]) + np.abs(prims[3]) + np.sqrt(prims[4]) / ma))
+    p = cases.hit_params(n, re=1000.0, ma=ma, dt=0.5 * (2.0 * math.pi / n) / vmax)
+    ref, out = _run_pair(p, cases.hit_coords(n), prims, 5)
+    np.testing.assert_array_equal(out[True], ref)
+    err = rel_l2(out[False], ref)
+    assert err < 1e-12, err

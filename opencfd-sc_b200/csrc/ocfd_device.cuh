@@ -171,6 +171,80 @@ __device__ __forceinline__ void split_llf(const Phys& ph, R g, R c, R d, R u, R 
   fm[4] = R(0.5) * (h0 * un - lamda0 * E0);
 }
 
+// The splittings for a sweep whose metric row has a single non-zero component,
+// the one along the sweep (box and 1-D grids; production build only): A is
+// that component, |grad xi| = |A| and the unit normal is sign(A) along DIR, so
+// the square root, the reciprocal and the products with the zero components of
+// the general forms above drop out (results move by rounding only).
+template <int DIR, typename R>
+__device__ __forceinline__ void split_sw_axis(const Phys& ph, R g, R c, R d, R u, R v, R w, R A, R* fp, R* fm) {
+  const R tmp1 = R(2) * (g - R(1));
+  const R tmp3 = R(ph.sw_tmp3);
+  const R ss = fabs(A);
+  const R cs = c * copysign(R(1), A);  // c ak_DIR
+  const R vs = A * (DIR == 0 ? u : (DIR == 1 ? v : w));
+  R E1 = vs, E2 = vs - c * ss, E3 = vs + c * ss;
+  R E1P = (E1 + fabs(E1)) * R(0.5), E2P = (E2 + fabs(E2)) * R(0.5), E3P = (E3 + fabs(E3)) * R(0.5);
+  R E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
+  R tmp0 = d * R(ph.inv_2g);
+  R uc1 = u, uc2 = u, vc1 = v, vc2 = v, wc1 = w, wc2 = w;
+  if (DIR == 0) {
+    uc1 = u - cs;
+    uc2 = u + cs;
+  } else if (DIR == 1) {
+    vc1 = v - cs;
+    vc2 = v + cs;
+  } else {
+    wc1 = w - cs;
+    wc2 = w + cs;
+  }
+  R vvc1 = (uc1 * uc1 + vc1 * vc1 + wc1 * wc1) * R(0.5);
+  R vvc2 = (uc2 * uc2 + vc2 * vc2 + wc2 * wc2) * R(0.5);
+  R vv = (g - R(1)) * (u * u + v * v + w * w);
+  R W2 = tmp3 * c * c;
+  fp[0] = tmp0 * (tmp1 * E1P + E2P + E3P);
+  fp[1] = tmp0 * (tmp1 * E1P * u + E2P * uc1 + E3P * uc2);
+  fp[2] = tmp0 * (tmp1 * E1P * v + E2P * vc1 + E3P * vc2);
+  fp[3] = tmp0 * (tmp1 * E1P * w + E2P * wc1 + E3P * wc2);
+  fp[4] = tmp0 * (E1P * vv + E2P * vvc1 + E3P * vvc2 + W2 * (E2P + E3P));
+  fm[0] = tmp0 * (tmp1 * E1M + E2M + E3M);
+  fm[1] = tmp0 * (tmp1 * E1M * u + E2M * uc1 + E3M * uc2);
+  fm[2] = tmp0 * (tmp1 * E1M * v + E2M * vc1 + E3M * vc2);
+  fm[3] = tmp0 * (tmp1 * E1M * w + E2M * wc1 + E3M * wc2);
+  fm[4] = tmp0 * (E1M * vv + E2M * vvc1 + E3M * vvc2 + W2 * (E2M + E3M));
+}
+
+template <int DIR, typename R>
+__device__ __forceinline__ void split_llf_axis(const Phys& ph, R g, R c, R d, R u, R v, R w, R A, R* fp, R* fm) {
+  const R tmp0 = R(ph.inv_g);
+  const R tmp1 = R(ph.inv_gm1);
+  const R un = A * (DIR == 0 ? u : (DIR == 1 ? v : w));
+  const R lamda0 = fabs(un) + fabs(A) * c;
+  const R p1 = tmp0 * d * c * c;
+  const R E0 = tmp1 * p1 + R(0.5) * d * (u * u + v * v + w * w);
+  const R h0 = E0 + p1;
+  const R Ap = A * p1;
+  fp[0] = R(0.5) * (d * un + lamda0 * d);
+  fp[1] = R(0.5) * (DIR == 0 ? d * u * un + Ap + lamda0 * d * u : d * u * un + lamda0 * d * u);
+  fp[2] = R(0.5) * (DIR == 1 ? d * v * un + Ap + lamda0 * d * v : d * v * un + lamda0 * d * v);
+  fp[3] = R(0.5) * (DIR == 2 ? d * w * un + Ap + lamda0 * d * w : d * w * un + lamda0 * d * w);
+  fp[4] = R(0.5) * (h0 * un + lamda0 * E0);
+  fm[0] = R(0.5) * (d * un - lamda0 * d);
+  fm[1] = R(0.5) * (DIR == 0 ? d * u * un + Ap - lamda0 * d * u : d * u * un - lamda0 * d * u);
+  fm[2] = R(0.5) * (DIR == 1 ? d * v * un + Ap - lamda0 * d * v : d * v * un - lamda0 * d * v);
+  fm[3] = R(0.5) * (DIR == 2 ? d * w * un + Ap - lamda0 * d * w : d * w * un - lamda0 * d * w);
+  fm[4] = R(0.5) * (h0 * un - lamda0 * E0);
+}
+
+// Metric row of sweep DIR (A?1 arrays 13 + 3 DIR .. 15 + 3 DIR) has its two
+// off-diagonal components identically +0.0.
+template <int DIR>
+__host__ __device__ __forceinline__ bool axis_aligned(unsigned int metzero) {
+  const int m0 = 13 + 3 * DIR;
+  const unsigned int off = (DIR == 0 ? 6u : (DIR == 1 ? 5u : 3u)) << m0;  // the two components other than DIR
+  return (metzero & off) == off;
+}
+
 // set_hybrid_scheme: OCFD_SetHybrid.f90:2-15
 __device__ __forceinline__ int hybrid_index(double R0, double t1, double t2) {
   if (R0 <= t1) return 1;

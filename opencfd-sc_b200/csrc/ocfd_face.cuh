@@ -287,6 +287,109 @@ __device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf
 __device__ __forceinline__ double xrcp(double a) { return __drcp_rn(a); }
 __device__ __forceinline__ float xrcp(float a) { return __frcp_rn(a); }
 
+// Characteristic basis of one face, production build: the rows of L = S and
+// R = S^-1 of flux_charteric (OCFD_inviscous_character.f90:216-248) applied
+// without forming the matrices.  AXS: the sweep's metric row has a single
+// non-zero component (box and 1-D grids), so n = s e_DIR with s its sign, and
+// the general construction gives l = s e_y, m = e_z (DIR 0), l = -s e_x, m = e_z
+// (DIR 1), l = -s e_x, m = -e_y (DIR 2): exact 0 and +-1 entries, whose terms
+// the projections and the back projection skip.  Derived quantities (V2, un,
+// ul, um, m) are recomputed where used, so that a face kept for the deferred
+// limiter pass holds only u, v, w, c and the basis.
+template <int DIR, bool AXS, typename R>
+struct CharBasis {
+  static constexpr int LI = DIR == 0 ? 1 : 0;  // AXS: the velocity component along l
+  static constexpr int MI = DIR == 2 ? 1 : 2;  // and along m
+  R u, v, w, c;
+  R n1, n2, n3, l1, l2, l3;  // AXS: n1 holds s, the others are unused
+
+  __device__ __forceinline__ void init(R u1, R v1, R w1, R c1, R a1, R a2, R a3) {
+    u = u1;
+    v = v1;
+    w = w1;
+    c = c1;
+    if constexpr (AXS) {
+      n1 = copysign(R(1), DIR == 0 ? a1 : (DIR == 1 ? a2 : a3));
+    } else {
+      const R rs = rsqrt(a1 * a1 + a2 * a2 + a3 * a3);
+      n1 = a1 * rs;
+      n2 = a2 * rs;
+      n3 = a3 * rs;
+      if (fabs(n3) <= fabs(n2)) {
+        const R rl = rsqrt(n1 * n1 + n2 * n2);
+        l1 = -n2 * rl;
+        l2 = n1 * rl;
+        l3 = R(0);
+      } else {
+        const R rl = rsqrt(n1 * n1 + n3 * n3);
+        l1 = -n3 * rl;
+        l3 = n1 * rl;
+        l2 = R(0);
+      }
+    }
+  }
+  __device__ __forceinline__ R vel(int q) const { return q == 0 ? u : (q == 1 ? v : w); }
+  __device__ __forceinline__ R sl() const { return DIR == 0 ? n1 : -n1; }  // AXS: the non-zero entry of l
+  __device__ __forceinline__ R V2() const { return (u * u + v * v + w * w) * R(0.5); }
+  __device__ __forceinline__ R un() const { return AXS ? n1 * vel(DIR) : u * n1 + v * n2 + w * n3; }
+  __device__ __forceinline__ R ul() const { return AXS ? sl() * vel(LI) : u * l1 + v * l2 + w * l3; }
+  __device__ __forceinline__ R um() const {
+    if constexpr (AXS) return DIR == 2 ? -v : w;
+    return u * (n2 * l3 - n3 * l2) + v * (n3 * l1 - n1 * l3) + w * (n1 * l2 - n2 * l1);
+  }
+  // c = L f for one point (rows 0, 3, 4 through A = (V2,-u,-v,-w,1).f and
+  // B = (un,-n).f: F0 - KK A and KK1 A +- X1 B)
+  __device__ __forceinline__ void proj(R f0, R f1, R f2, R f3, R f4, R KK, R KK1, R X1, R V2_, R un_, R ul_,
+                                       R um_, R* cc) const {
+    const R A = V2_ * f0 - u * f1 - v * f2 - w * f3 + f4;
+    cc[0] = f0 - KK * A;
+    if constexpr (AXS) {
+      const R f[3] = {f1, f2, f3};
+      const R B = un_ * f0 - n1 * f[DIR];
+      cc[1] = sl() * f[LI] - ul_ * f0;
+      cc[2] = (DIR == 2 ? -f[MI] : f[MI]) - um_ * f0;
+      cc[3] = KK1 * A + X1 * B;
+      cc[4] = KK1 * A - X1 * B;
+    } else {
+      const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+      const R B = un_ * f0 - n1 * f1 - n2 * f2 - n3 * f3;
+      cc[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul_ * f0;
+      cc[2] = m1 * f1 + m2 * f2 + m3 * f3 - um_ * f0;
+      cc[3] = KK1 * A + X1 * B;
+      cc[4] = KK1 * A - X1 * B;
+    }
+  }
+  // hh = R h0 (OCFD_inviscous_character.f90:284-288), H = V2 + c^2/(gamma-1)
+  __device__ __forceinline__ void back(const R* h0, R* hh, R inv_gm1) const {
+    const R V2_ = V2(), un_ = un(), ul_ = ul(), um_ = um();
+    const R H = V2_ + c * c * inv_gm1;
+    hh[0] = h0[0] + h0[3] + h0[4];
+    if constexpr (AXS) {
+      const R cs = c * n1;
+      R q[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const R vk = vel(k);
+        if (k == DIR)
+          q[k] = vk * h0[0] + (vk - cs) * h0[3] + (vk + cs) * h0[4];
+        else if (k == LI)
+          q[k] = vk * h0[0] + sl() * h0[1] + vk * h0[3] + vk * h0[4];
+        else
+          q[k] = vk * h0[0] + (DIR == 2 ? -h0[2] : h0[2]) + vk * h0[3] + vk * h0[4];
+      }
+      hh[1] = q[0];
+      hh[2] = q[1];
+      hh[3] = q[2];
+    } else {
+      const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+      hh[1] = u * h0[0] + l1 * h0[1] + m1 * h0[2] + (u - c * n1) * h0[3] + (u + c * n1) * h0[4];
+      hh[2] = v * h0[0] + l2 * h0[1] + m2 * h0[2] + (v - c * n2) * h0[3] + (v + c * n2) * h0[4];
+      hh[3] = w * h0[0] + l3 * h0[1] + m3 * h0[2] + (w - c * n3) * h0[3] + (w + c * n3) * h0[4];
+    }
+    hh[4] = V2_ * h0[0] + ul_ * h0[1] + um_ * h0[2] + (H - c * un_) * h0[3] + (H + c * un_) * h0[4];
+  }
+};
+
 // One queued limiter evaluation (OCFD_inviscous_character.f90:205-248 for the
 // face state and row r of the left eigenvector matrix, :256-270 for the
 // projection, OCFD_Schemes_1.f90:212-224 for the limiter): the face whose
@@ -295,25 +398,40 @@ __device__ __forceinline__ float xrcp(float a) { return __frcp_rn(a); }
 // rounded operations, so that every kernel that inlines it produces the same
 // bits.
 // Window element (var, stencil point q) at wb[var * VS + (var >= 5 ? GAP : 0) + q * QS].
-template <typename R, int VS, int QS, int GAP>
+// AXS: the axis-aligned basis of CharBasis (n = s e_DIR, l and m of exact 0 and
+// +-1 entries).
+template <typename R, int VS, int QS, int GAP, int DIR = 0, bool AXS = false>
 __device__ __forceinline__ R lim_eval(const R* wb, int r, int minus, R mid, R gm1) {
   auto mean = [&](int var) {
     return xmul(xadd(wb[var * VS + GAP + 3 * QS], wb[var * VS + GAP + 4 * QS]), R(0.5));  // var >= 10
   };
-  const R u1 = mean(10), v1 = mean(11), w1 = mean(12), c1 = mean(13), a1 = mean(14), a2 = mean(15), a3 = mean(16);
-  const R rs = rsqrt(xfma(a3, a3, xfma(a2, a2, xmul(a1, a1))));
-  const R n1 = xmul(a1, rs), n2 = xmul(a2, rs), n3 = xmul(a3, rs);
-  R l1, l2, l3;
-  if (fabs(n3) <= fabs(n2)) {
-    const R rl = rsqrt(xfma(n2, n2, xmul(n1, n1)));
-    l1 = -xmul(n2, rl);
-    l2 = xmul(n1, rl);
+  const R u1 = mean(10), v1 = mean(11), w1 = mean(12), c1 = mean(13);
+  R n1, n2, n3, l1, l2, l3;
+  if constexpr (AXS) {
+    const R s = copysign(R(1), mean(14 + DIR));
+    n1 = DIR == 0 ? s : R(0);
+    n2 = DIR == 1 ? s : R(0);
+    n3 = DIR == 2 ? s : R(0);
+    l1 = DIR == 0 ? R(0) : -s;
+    l2 = DIR == 0 ? s : R(0);
     l3 = R(0);
   } else {
-    const R rl = rsqrt(xfma(n3, n3, xmul(n1, n1)));
-    l1 = -xmul(n3, rl);
-    l3 = xmul(n1, rl);
-    l2 = R(0);
+    const R a1 = mean(14), a2 = mean(15), a3 = mean(16);
+    const R rs = rsqrt(xfma(a3, a3, xfma(a2, a2, xmul(a1, a1))));
+    n1 = xmul(a1, rs);
+    n2 = xmul(a2, rs);
+    n3 = xmul(a3, rs);
+    if (fabs(n3) <= fabs(n2)) {
+      const R rl = rsqrt(xfma(n2, n2, xmul(n1, n1)));
+      l1 = -xmul(n2, rl);
+      l2 = xmul(n1, rl);
+      l3 = R(0);
+    } else {
+      const R rl = rsqrt(xfma(n3, n3, xmul(n1, n1)));
+      l1 = -xmul(n3, rl);
+      l3 = xmul(n1, rl);
+      l2 = R(0);
+    }
   }
   R c[5];
   if (r == 1) {
@@ -380,7 +498,11 @@ __device__ __forceinline__ R lim_eval(const R* wb, int r, int minus, R mid, R gm
 // TMA: the eight input arrays were staged in shared memory by the caller
 // (tile: TmaBox slots of d, u, v, w, T, A1, A2, A3; toff: offset of the first
 // stencil point / pencil in the tile's innermost dimension).
-template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S, bool TMA = false>
+// AXS (production build, ALLIN sweeps): the sweep's metric row has a single
+// non-zero component (axis_aligned); the splitting and the characteristic
+// basis use the axis-aligned forms.
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S, bool TMA = false,
+          bool AXS = false>
 __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, const int by, const int bz, R* sm,
                                           const S* tile = nullptr, int toff = 0) {
   constexpr int LT = TF + 7;
@@ -460,9 +582,15 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       w = R(tile[3 * B::SLOT_ELEMS + e]);
       T = R(tile[4 * B::SLOT_ELEMS + e]);
       const int m0 = 13 + 3 * DIR;
-      A1 = ((ph.metzero >> m0) & 1u) ? R(0) : R(tile[5 * B::SLOT_ELEMS + e]);
-      A2 = ((ph.metzero >> (m0 + 1)) & 1u) ? R(0) : R(tile[6 * B::SLOT_ELEMS + e]);
-      A3 = ((ph.metzero >> (m0 + 2)) & 1u) ? R(0) : R(tile[7 * B::SLOT_ELEMS + e]);
+      if constexpr (AXS) {
+        A1 = DIR == 0 ? R(tile[5 * B::SLOT_ELEMS + e]) : R(0);
+        A2 = DIR == 1 ? R(tile[6 * B::SLOT_ELEMS + e]) : R(0);
+        A3 = DIR == 2 ? R(tile[7 * B::SLOT_ELEMS + e]) : R(0);
+      } else {
+        A1 = ((ph.metzero >> m0) & 1u) ? R(0) : R(tile[5 * B::SLOT_ELEMS + e]);
+        A2 = ((ph.metzero >> (m0 + 1)) & 1u) ? R(0) : R(tile[6 * B::SLOT_ELEMS + e]);
+        A3 = ((ph.metzero >> (m0 + 2)) & 1u) ? R(0) : R(tile[7 * B::SLOT_ELEMS + e]);
+      }
     } else if (ok) {
       long long h = G.ih(i, j, k) + (long long)gl * hs;
       d = R(__ldg(a.d + h));
@@ -478,9 +606,15 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         w = R(__ldg(a.w + h));
         T = R(__ldg(a.T + h));
       }
-      A1 = met_at<R>(ph, 13 + 3 * DIR, a.A1, h);
-      A2 = met_at<R>(ph, 14 + 3 * DIR, a.A2, h);
-      A3 = met_at<R>(ph, 15 + 3 * DIR, a.A3, h);
+      if constexpr (AXS) {
+        A1 = DIR == 0 ? R(__ldg(a.A1 + h)) : R(0);
+        A2 = DIR == 1 ? R(__ldg(a.A2 + h)) : R(0);
+        A3 = DIR == 2 ? R(__ldg(a.A3 + h)) : R(0);
+      } else {
+        A1 = met_at<R>(ph, 13 + 3 * DIR, a.A1, h);
+        A2 = met_at<R>(ph, 14 + 3 * DIR, a.A2, h);
+        A3 = met_at<R>(ph, 15 + 3 * DIR, a.A3, h);
+      }
     }
 #if OCFD_FEWER_DIVS
     const R c = sqrt(T) * R(ph.inv_ma);
@@ -488,10 +622,18 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
     const R c = sqrt(T) / ma;  // cc: OCFD_inviscous.f90:67
 #endif
     R fp[5], fm[5];
-    if (a.split == 1)
-      split_sw(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
-    else
-      split_llf(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+    if constexpr (AXS) {
+      const R Ad = DIR == 0 ? A1 : (DIR == 1 ? A2 : A3);
+      if (a.split == 1)
+        split_sw_axis<DIR>(ph, gam, c, d, u, v, w, Ad, fp, fm);
+      else
+        split_llf_axis<DIR>(ph, gam, c, d, u, v, w, Ad, fp, fm);
+    } else {
+      if (a.split == 1)
+        split_sw(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+      else
+        split_llf(ph, gam, c, d, u, v, w, A1, A2, A3, fp, fm);
+    }
     if constexpr (PS > 1) {
       // the point's record in 16-byte stores (the unused slots get zeros)
       float4* r4 = reinterpret_cast<float4*>(sm + PI(l, p) * PS);
@@ -535,8 +677,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   int djb = 0;
   bool dpend = false;
   long long dfo = 0;
-  R bu = R(0), bv = R(0), bw = R(0), bc = R(0), bn1 = R(0), bn2 = R(0), bn3 = R(0), bl1 = R(0), bl2 = R(0),
-    bl3 = R(0);
+  CharBasis<DIR, AXS, R> dcb{};
 
   for (int t = threadIdx.x; t < NP * TF; t += blockDim.x) {
     int f, p;
@@ -660,39 +801,41 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         const R v1 = (W(11, 3) + W(11, 4)) * R(0.5);
         const R w1 = (W(12, 3) + W(12, 4)) * R(0.5);
         const R c1 = (W(13, 3) + W(13, 4)) * R(0.5);
-        const R a1 = (W(14, 3) + W(14, 4)) * R(0.5);
-        const R a2 = (W(15, 3) + W(15, 4)) * R(0.5);
-        const R a3 = (W(16, 3) + W(16, 4)) * R(0.5);
+        const R a1 = (AXS && DIR != 0) ? R(0) : (W(14, 3) + W(14, 4)) * R(0.5);
+        const R a2 = (AXS && DIR != 1) ? R(0) : (W(15, 3) + W(15, 4)) * R(0.5);
+        const R a3 = (AXS && DIR != 2) ? R(0) : (W(16, 3) + W(16, 4)) * R(0.5);
         // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
 #if OCFD_FEWER_DIVS
-        const R rs = rsqrt(a1 * a1 + a2 * a2 + a3 * a3);
-        const R n1 = a1 * rs, n2 = a2 * rs, n3 = a3 * rs;
+        CharBasis<DIR, AXS, R> cb;
+        cb.init(u1, v1, w1, c1, a1, a2, a3);
+        const R V2 = cb.V2(), un = cb.un(), ul = cb.ul(), um = cb.um();
+        const R rc = R(1) / c1;
+        const R KK = (R(ph.gamma) - R(1)) * (rc * rc);
+        const R KK1 = KK * R(0.5);
+        const R X1 = R(0.5) * rc;
+        // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
+        // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
+        auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
+          cb.proj(f0, f1, f2, f3, f4, KK, KK1, X1, V2, un, ul, um, c);
+        };
+        auto proj5 = [&](int vb, int q, R* c) {
+          R f4[4];
+          W4(vb, q, f4);
+          proj5v(f4[0], f4[1], f4[2], f4[3], W(vb + 4, q), c);
+        };
 #else
         R ss = sqrt(a1 * a1 + a2 * a2 + a3 * a3);
         const R n1 = a1 / ss, n2 = a2 / ss, n3 = a3 / ss;
-#endif
         R l1, l2, l3;
         if (fabs(n3) <= fabs(n2)) {
-#if OCFD_FEWER_DIVS
-          const R rl = rsqrt(n1 * n1 + n2 * n2);
-          l1 = -n2 * rl;
-          l2 = n1 * rl;
-#else
           ss = sqrt(n1 * n1 + n2 * n2);
           l1 = -n2 / ss;
           l2 = n1 / ss;
-#endif
           l3 = R(0);
         } else {
-#if OCFD_FEWER_DIVS
-          const R rl = rsqrt(n1 * n1 + n3 * n3);
-          l1 = -n3 * rl;
-          l3 = n1 * rl;
-#else
           ss = sqrt(n1 * n1 + n3 * n3);
           l1 = -n3 / ss;
           l3 = n1 / ss;
-#endif
           l2 = R(0);
         }
         const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
@@ -700,16 +843,9 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         const R ul = u1 * l1 + v1 * l2 + w1 * l3;
         const R um = u1 * m1 + v1 * m2 + w1 * m3;
         const R V2 = (u1 * u1 + v1 * v1 + w1 * w1) * R(0.5);
-#if OCFD_FEWER_DIVS
-        const R rc = R(1) / c1;
-        const R KK = (R(ph.gamma) - R(1)) * (rc * rc);
-        const R KK1 = KK * R(0.5);
-        const R X1 = R(0.5) * rc;
-#else
         const R KK = (R(ph.gamma) - R(1)) / (c1 * c1);
         const R KK1 = KK * R(0.5);
         const R X1 = R(1) / (R(2) * c1);
-#endif
         const R L[5][5] = {{R(1) - KK * V2, KK * u1, KK * v1, KK * w1, -KK},
                            {-ul, l1, l2, l3, R(0)},
                            {-um, m1, m2, m3, R(0)},
@@ -721,22 +857,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           if (r == 1 || r == 2) return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3;
           return L[r][0] * f0 + L[r][1] * f1 + L[r][2] * f2 + L[r][3] * f3 + L[r][4] * W(vb + 4, q);
         };
-        // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
-        // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
-        auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
-          const R A = V2 * f0 - u1 * f1 - v1 * f2 - w1 * f3 + f4;
-          const R B = un * f0 - n1 * f1 - n2 * f2 - n3 * f3;
-          c[0] = f0 - KK * A;
-          c[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul * f0;
-          c[2] = m1 * f1 + m2 * f2 + m3 * f3 - um * f0;
-          c[3] = KK1 * A + X1 * B;
-          c[4] = KK1 * A - X1 * B;
-        };
-        auto proj5 = [&](int vb, int q, R* c) {
-          R f4[4];
-          W4(vb, q, f4);
-          proj5v(f4[0], f4[1], f4[2], f4[3], W(vb + 4, q), c);
-        };
+#endif
         R h0[5];
         if (SCHEME == SCH_OMP6 && inner) {
           // OMP6, interior face: the linear part of hh_OMP6P/M (OCFD_Schemes_1.f90:211,244) is
@@ -844,16 +965,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           }
           dpend = true;
           dfo = fo;
-          bu = u1;
-          bv = v1;
-          bw = w1;
-          bc = c1;
-          bn1 = n1;
-          bn2 = n2;
-          bn3 = n3;
-          bl1 = l1;
-          bl2 = l2;
-          bl3 = l3;
+          dcb = cb;
           continue;
 #else
           {
@@ -968,12 +1080,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           }
         }
         // ---- back to physical space, hh = R h0 (:284-288); R = S^-1 (:244-248)
+#if OCFD_FEWER_DIVS
+        cb.back(h0, hh, R(ph.inv_gm1));
+#else
         const R H = V2 + R(1) / KK;
         hh[0] = h0[0] + h0[3] + h0[4];
         hh[1] = u1 * h0[0] + l1 * h0[1] + m1 * h0[2] + (u1 - c1 * n1) * h0[3] + (u1 + c1 * n1) * h0[4];
         hh[2] = v1 * h0[0] + l2 * h0[1] + m2 * h0[2] + (v1 - c1 * n2) * h0[3] + (v1 + c1 * n2) * h0[4];
         hh[3] = w1 * h0[0] + l3 * h0[1] + m3 * h0[2] + (w1 - c1 * n3) * h0[3] + (w1 + c1 * n3) * h0[4];
         hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - c1 * un) * h0[3] + (H + c1 * un) * h0[4];
+#endif
       }
     }
 #pragma unroll
@@ -985,7 +1101,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
     const R gm1 = R(ph.gamma) - R(1);
     for (int e = threadIdx.x; e < nj; e += blockDim.x) {
       const int tag = jtag[e];
-      jv[e] = lim_eval<R, VS, QS, GAP>(sm + (tag >> 4), (tag >> 1) & 7, tag & 1, jv[e], gm1);
+      jv[e] = lim_eval<R, VS, QS, GAP, DIR, AXS>(sm + (tag >> 4), (tag >> 1) & 7, tag & 1, jv[e], gm1);
     }
     __syncthreads();
     if (dpend) {
@@ -1001,18 +1117,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       R h0[5];
 #pragma unroll
       for (int r = 0; r < 5; r++) h0[r] = dP[r] + dM[r];
-      const R m1 = bn2 * bl3 - bn3 * bl2, m2 = bn3 * bl1 - bn1 * bl3, m3 = bn1 * bl2 - bn2 * bl1;
-      const R un = bu * bn1 + bv * bn2 + bw * bn3;
-      const R ul = bu * bl1 + bv * bl2 + bw * bl3;
-      const R um = bu * m1 + bv * m2 + bw * m3;
-      const R V2 = (bu * bu + bv * bv + bw * bw) * R(0.5);
-      const R H = V2 + bc * bc * R(ph.inv_gm1);
       R hh[5];
-      hh[0] = h0[0] + h0[3] + h0[4];
-      hh[1] = bu * h0[0] + bl1 * h0[1] + m1 * h0[2] + (bu - bc * bn1) * h0[3] + (bu + bc * bn1) * h0[4];
-      hh[2] = bv * h0[0] + bl2 * h0[1] + m2 * h0[2] + (bv - bc * bn2) * h0[3] + (bv + bc * bn2) * h0[4];
-      hh[3] = bw * h0[0] + bl3 * h0[1] + m3 * h0[2] + (bw - bc * bn3) * h0[3] + (bw + bc * bn3) * h0[4];
-      hh[4] = V2 * h0[0] + ul * h0[1] + um * h0[2] + (H - bc * un) * h0[3] + (H + bc * un) * h0[4];
+      dcb.back(h0, hh, R(ph.inv_gm1));
 #pragma unroll
       for (int m = 0; m < 5; m++) out[dfo + (long long)m * a.fs] = hh[m];
     }
@@ -1036,11 +1142,11 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #define OCFD_FACE_BOUNDS                                                                      \
   __launch_bounds__(OCFD_FACE_NT, (OCFD_FACE_NT == 128 && sizeof(R) == 8) ? OCFD_FACE64_MINB128 \
                                                                           : OCFD_FACE_MINB * 256 / OCFD_FACE_NT)
-template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S, bool AXS = false>
 __global__ void OCFD_FACE_BOUNDS k_face(FaceArgs<S> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR, CHAR, SCHEME>::NP, FaceTile<DIR, CHAR, SCHEME>::TF, R, S>(
-      a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
+  face_body<DIR, CHAR, SCHEME, ALLIN, FaceTile<DIR, CHAR, SCHEME>::NP, FaceTile<DIR, CHAR, SCHEME>::TF, R, S, false,
+            AXS>(a, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<R*>(smem_raw));
 }
 
 // Batched launch: the blocks of all instances in one 1-D grid; each block finds
@@ -1052,13 +1158,20 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<Fac
   __shared__ __align__(16) FaceArgs<S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
-  face_body<DIR, CHAR, SCHEME, true, FaceTileV<DIR, V>::NP, FaceTileV<DIR, V>::TF, R, S>(
-      batch_args(b, q, &sa), bx, by, bz, reinterpret_cast<R*>(smem_raw));
+  const FaceArgs<S>& A = batch_args(b, q, &sa);
+  // the member's own sweep variant, as its single-instance launch would choose
+  // it (batched and single results are the same bits)
+  if (OCFD_FEWER_DIVS && axis_aligned<DIR>(A.ph.metzero))
+    face_body<DIR, CHAR, SCHEME, true, FaceTileV<DIR, V>::NP, FaceTileV<DIR, V>::TF, R, S, false,
+              OCFD_FEWER_DIVS != 0>(A, bx, by, bz, reinterpret_cast<R*>(smem_raw));
+  else
+    face_body<DIR, CHAR, SCHEME, true, FaceTileV<DIR, V>::NP, FaceTileV<DIR, V>::TF, R, S>(
+        A, bx, by, bz, reinterpret_cast<R*>(smem_raw));
 }
 
 // Single-instance sweep of a periodic direction with the input tiles staged by
 // TMA (the arithmetic is that of k_face).
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false>
 __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
@@ -1108,7 +1221,7 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
     }
     return;
   }
-  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true>(a, bx, by, bz, sm, tile, toff);
+  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true, AXS>(a, bx, by, bz, sm, tile, toff);
 }
 
 template <int DIR, bool CHAR, int NP, int TF, typename R>
@@ -1120,11 +1233,11 @@ constexpr size_t face_smem() {
 }
 
 // ---------------------------------------------------------------------------
-template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S>
+template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S, bool AXS = false>
 static cudaError_t launch_face_t(const FaceArgs<S>& a, cudaStream_t st) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   constexpr size_t smem = face_smem<DIR, CHAR, NP, TF, R>();
-  auto kern = k_face<DIR, CHAR, SCHEME, ALLIN, R, S>;
+  auto kern = k_face<DIR, CHAR, SCHEME, ALLIN, R, S, AXS>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<face_grid<DIR, NP, TF>(a), NP * TF, smem, st>>>(a);
   return cudaGetLastError();
@@ -1183,12 +1296,12 @@ inline bool tma_strides_ok(const Grid& g) {
   return ((long long)g.nxh * sizeof(S)) % 16 == 0 && ((long long)g.nxh * g.nyh * sizeof(S)) % 16 == 0;
 }
 
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S>
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false>
 static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
   constexpr size_t smem = 128 + 8 * (size_t)B::SLOT + face_smem<DIR, CHAR, NP, TF, R>();
-  auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S>;
+  auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S, AXS>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   FaceTmaMaps tm;
   const S* arr[8] = {a.d, a.u, a.v, a.w, a.T, a.A1, a.A2, a.A3};
@@ -1198,37 +1311,38 @@ static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// One (direction, form, scheme) combination: the TMA-staged sweep for FP64
+// periodic directions (measured 1-3% faster at 256^3; the FP32 sweeps, four
+// blocks per SM, are as fast or faster with plain loads), the axis-aligned
+// variant when the metric row allows it (production build).  An empty grid
+// asks for the shared-memory attribute of every variant instead.
+template <int D, bool C, int SC, typename R, typename S>
+static cudaError_t launch_face_dc(const FaceArgs<S>& a, cudaStream_t st) {
+  constexpr bool kAx = OCFD_FEWER_DIVS != 0;
+  if (a.g.n == 0) {
+    cudaError_t e = launch_face_t<D, C, SC, false, R, S>(a, st);
+    if (e == cudaSuccess) e = launch_face_t<D, C, SC, true, R, S>(a, st);
+    if (kAx && e == cudaSuccess) e = launch_face_t<D, C, SC, true, R, S, kAx>(a, st);
+    if constexpr (sizeof(S) == 8) {
+      if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S>(a, st);
+      if (kAx && e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, kAx>(a, st);
+    }
+    return e;
+  }
+  const bool allin = a.ph.periodic[D] != 0;
+  if (!allin) return launch_face_t<D, C, SC, false, R, S>(a, st);
+  const bool ax = kAx && axis_aligned<D>(a.ph.metzero);
+  if constexpr (sizeof(S) == 8) {
+    if (!a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g))
+      return ax ? launch_face_tma_t<D, C, SC, R, S, kAx>(a, st) : launch_face_tma_t<D, C, SC, R, S>(a, st);
+  }
+  return ax ? launch_face_t<D, C, SC, true, R, S, kAx>(a, st) : launch_face_t<D, C, SC, true, R, S>(a, st);
+}
+
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st) {
-  const bool allin = a.ph.periodic[dir] != 0;
-  // TMA staging for the FP64 sweeps (measured 1-3% faster at 256^3); the FP32
-  // sweeps, four blocks per SM, are as fast or faster with plain loads
-  if constexpr (sizeof(S) == 8)
-  if (allin && (a.g.n == 0 || (!a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g)))) {
-    // set-up (empty grid) registers both kernels; launches take the TMA path
-#define OCFD_FACE_TMA_CASE(D, C, SC)                                                        \
-    if (dir == D && chr == C && scheme == SC) {                                               \
-      cudaError_t e = launch_face_tma_t<D, C, SC, R, S>(a, st);                               \
-      if (a.g.n != 0 || e != cudaSuccess) return e;                                           \
-    }
-#define OCFD_FACE_TMA_SCHEMES(D, C) \
-    OCFD_FACE_TMA_CASE(D, C, SCH_WENO5) \
-    OCFD_FACE_TMA_CASE(D, C, SCH_WENO7) \
-    OCFD_FACE_TMA_CASE(D, C, SCH_OMP6)  \
-    OCFD_FACE_TMA_CASE(D, C, SCH_UD7L)  \
-    OCFD_FACE_TMA_CASE(D, C, SCH_HYBRID)
-    OCFD_FACE_TMA_SCHEMES(0, false)
-    OCFD_FACE_TMA_SCHEMES(1, false)
-    OCFD_FACE_TMA_SCHEMES(2, false)
-    OCFD_FACE_TMA_SCHEMES(0, true)
-    OCFD_FACE_TMA_SCHEMES(1, true)
-    OCFD_FACE_TMA_SCHEMES(2, true)
-#undef OCFD_FACE_TMA_SCHEMES
-#undef OCFD_FACE_TMA_CASE
-  }
-#define OCFD_FACE_CASE(D, C, SC)                                                    \
-  if (dir == D && chr == C && scheme == SC)                                         \
-    return allin ? launch_face_t<D, C, SC, true, R, S>(a, st) : launch_face_t<D, C, SC, false, R, S>(a, st);
+#define OCFD_FACE_CASE(D, C, SC) \
+  if (dir == D && chr == C && scheme == SC) return launch_face_dc<D, C, SC, R, S>(a, st);
 #define OCFD_FACE_SCHEMES(D, C)         \
   OCFD_FACE_CASE(D, C, SCH_WENO5)       \
   OCFD_FACE_CASE(D, C, SCH_WENO7)       \

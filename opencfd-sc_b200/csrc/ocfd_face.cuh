@@ -504,7 +504,7 @@ __device__ __forceinline__ R lim_eval(const R* wb, int r, int minus, R mid, R gm
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, int NP, int TF, typename R, typename S, bool TMA = false,
           bool AXS = false>
 __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, const int by, const int bz, R* sm,
-                                          const S* tile = nullptr, int toff = 0) {
+                                          const S* tile = nullptr, int toff = 0, R* qbase = nullptr) {
   constexpr int LT = TF + 7;
   // shared memory (face_ps).  Records (PS > 1): F+ and F- each start on a
   // 16-byte boundary (GAP unused values after F+), so that four components of
@@ -553,7 +553,9 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   // component * 2 + side), the entry count
   constexpr bool DEFER = CHAR && SCHEME == SCH_OMP6 && OCFD_FEWER_DIVS;
   constexpr int JC = LimQueue<NP * TF>::CAP;  // one face per thread: blockDim.x == NP * TF
-  R* const jv = sm + (PS > 1 ? PS : 17) * NP * LT;
+  // (qbase: the caller's queue, which may share memory with the staged input
+  // tile -- dead after phase 1; the entry count lies past that tile)
+  R* const jv = qbase ? qbase : sm + (PS > 1 ? PS : 17) * NP * LT;
   int* const jtag = reinterpret_cast<int*>(jv + JC);
   int* const jn = jtag + JC;
   if (DEFER && threadIdx.x == 0) *jn = 0;
@@ -1125,6 +1127,32 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
   }
 }
 
+template <int DIR, bool CHAR, int NP, int TF, typename R>
+constexpr size_t face_smem_points() {
+  // split fluxes (+ face state)
+  return (size_t)(face_ps<DIR, CHAR, R>() > 1 ? face_ps<DIR, CHAR, R>() : (CHAR ? 17 : 10)) * NP * (TF + 7) *
+         sizeof(R);
+}
+template <int DIR, bool CHAR, int NP, int TF, typename R>
+constexpr size_t face_smem() {
+  // (+ the limiter queue)
+  return face_smem_points<DIR, CHAR, NP, TF, R>() + (CHAR ? LimQueue<NP * TF>::template bytes<R>() : 0);
+}
+// TMA sweeps: the limiter queue shares memory with the eight staged input
+// tiles (read only in phase 1, the queue is used after phase 1's barrier) when
+// its entry count -- written before phase 1 -- lies past them.
+template <int DIR, bool CHAR, int SCHEME, int NP, int TF, typename R, typename S>
+struct FaceTmaSmem {
+  using B = TmaBox<DIR, NP, TF, S>;
+  static constexpr size_t TILE = 8 * (size_t)B::SLOT;
+  static constexpr size_t QB = LimQueue<NP * TF>::template bytes<R>();
+  static constexpr size_t COUNT_AT = (size_t)LimQueue<NP * TF>::CAP * (sizeof(R) + sizeof(int));
+  static constexpr bool ALIAS = CHAR && SCHEME == SCH_OMP6 && OCFD_FEWER_DIVS && COUNT_AT >= TILE;
+  static constexpr size_t UNION = ALIAS ? (TILE > QB ? TILE : QB) : TILE;  // before the staged points
+  static constexpr size_t BYTES =
+      128 + UNION + (ALIAS ? face_smem_points<DIR, CHAR, NP, TF, R>() : face_smem<DIR, CHAR, NP, TF, R>());
+};
+
 // Minimum resident blocks per SM.  FP64: two (<= 128 registers) measured
 // faster than one.  FP32: four (<= 64 registers) -- 17% faster than two on the
 // characteristic OMP6 sweeps at 256^3 despite a few spilled registers, equal on
@@ -1139,9 +1167,13 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #define OCFD_FACE64_MINB128 4  // FP64, 128-thread tiles: 4 blocks (128 registers); 5 (96
                                // registers) measured 2% faster on x, 8% slower on y and z
 #endif
-#define OCFD_FACE_BOUNDS                                                                      \
-  __launch_bounds__(OCFD_FACE_NT, (OCFD_FACE_NT == 128 && sizeof(R) == 8) ? OCFD_FACE64_MINB128 \
-                                                                          : OCFD_FACE_MINB * 256 / OCFD_FACE_NT)
+#ifndef OCFD_FACE64_MINB128_AX
+#define OCFD_FACE64_MINB128_AX 5  // the axis-aligned variants (about 110 registers at 4 blocks)
+#endif
+#define OCFD_FACE_BOUNDS                                                                                     \
+  __launch_bounds__(OCFD_FACE_NT,                                                                            \
+                    (OCFD_FACE_NT == 128 && sizeof(R) == 8) ? (AXS ? OCFD_FACE64_MINB128_AX : OCFD_FACE64_MINB128) \
+                                                            : OCFD_FACE_MINB * 256 / OCFD_FACE_NT)
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S, bool AXS = false>
 __global__ void OCFD_FACE_BOUNDS k_face(FaceArgs<S> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1180,8 +1212,10 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
   // TMA destinations start on 128-byte boundaries (128 bytes of the launch's
   // dynamic shared memory are reserved for this rounding)
   unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127u)) & 127u);
+  using L = FaceTmaSmem<DIR, CHAR, SCHEME, NP, TF, R, S>;
   S* tile = reinterpret_cast<S*>(base);
-  R* sm = reinterpret_cast<R*>(base + 8 * B::SLOT);
+  R* sm = reinterpret_cast<R*>(base + L::UNION);
+  R* qbase = L::ALIAS ? reinterpret_cast<R*>(base) : nullptr;
   const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
   const int g0 = a.fbeg + (DIR == 0 ? bx : by) * TF;  // first face; its stencil starts at g0 - 3
   const int pbase = (DIR == 0 ? by : bx) * NP;
@@ -1221,16 +1255,9 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
     }
     return;
   }
-  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true, AXS>(a, bx, by, bz, sm, tile, toff);
+  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true, AXS>(a, bx, by, bz, sm, tile, toff, qbase);
 }
 
-template <int DIR, bool CHAR, int NP, int TF, typename R>
-constexpr size_t face_smem() {
-  // split fluxes (+ face state and the limiter queue)
-  return (size_t)(face_ps<DIR, CHAR, R>() > 1 ? face_ps<DIR, CHAR, R>() : (CHAR ? 17 : 10)) * NP * (TF + 7) *
-             sizeof(R) +
-         (CHAR ? LimQueue<NP * TF>::template bytes<R>() : 0);
-}
 
 // ---------------------------------------------------------------------------
 template <int DIR, bool CHAR, int SCHEME, bool ALLIN, typename R, typename S, bool AXS = false>
@@ -1300,7 +1327,7 @@ template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = fal
 static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
-  constexpr size_t smem = 128 + 8 * (size_t)B::SLOT + face_smem<DIR, CHAR, NP, TF, R>();
+  constexpr size_t smem = FaceTmaSmem<DIR, CHAR, SCHEME, NP, TF, R, S>::BYTES;
   auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S, AXS>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   FaceTmaMaps tm;

@@ -311,82 +311,95 @@ struct CharBasis {
     if constexpr (AXS) {
       n1 = copysign(R(1), DIR == 0 ? a1 : (DIR == 1 ? a2 : a3));
     } else {
-      const R rs = rsqrt(a1 * a1 + a2 * a2 + a3 * a3);
-      n1 = a1 * rs;
-      n2 = a2 * rs;
-      n3 = a3 * rs;
+      const R rs = rsqrt(xfma(a3, a3, xfma(a2, a2, xmul(a1, a1))));
+      n1 = xmul(a1, rs);
+      n2 = xmul(a2, rs);
+      n3 = xmul(a3, rs);
       if (fabs(n3) <= fabs(n2)) {
-        const R rl = rsqrt(n1 * n1 + n2 * n2);
-        l1 = -n2 * rl;
-        l2 = n1 * rl;
+        const R rl = rsqrt(xfma(n2, n2, xmul(n1, n1)));
+        l1 = -xmul(n2, rl);
+        l2 = xmul(n1, rl);
         l3 = R(0);
       } else {
-        const R rl = rsqrt(n1 * n1 + n3 * n3);
-        l1 = -n3 * rl;
-        l3 = n1 * rl;
+        const R rl = rsqrt(xfma(n3, n3, xmul(n1, n1)));
+        l1 = -xmul(n3, rl);
+        l3 = xmul(n1, rl);
         l2 = R(0);
       }
     }
   }
   __device__ __forceinline__ R vel(int q) const { return q == 0 ? u : (q == 1 ? v : w); }
   __device__ __forceinline__ R sl() const { return DIR == 0 ? n1 : -n1; }  // AXS: the non-zero entry of l
-  __device__ __forceinline__ R V2() const { return (u * u + v * v + w * w) * R(0.5); }
-  __device__ __forceinline__ R un() const { return AXS ? n1 * vel(DIR) : u * n1 + v * n2 + w * n3; }
-  __device__ __forceinline__ R ul() const { return AXS ? sl() * vel(LI) : u * l1 + v * l2 + w * l3; }
+  // m = n x l
+  __device__ __forceinline__ R m1() const { return xfma(n2, l3, -xmul(n3, l2)); }
+  __device__ __forceinline__ R m2() const { return xfma(n3, l1, -xmul(n1, l3)); }
+  __device__ __forceinline__ R m3() const { return xfma(n1, l2, -xmul(n2, l1)); }
+  __device__ __forceinline__ R V2() const { return xmul(xfma(w, w, xfma(v, v, xmul(u, u))), R(0.5)); }
+  __device__ __forceinline__ R un() const {
+    return AXS ? xmul(n1, vel(DIR)) : xfma(w, n3, xfma(v, n2, xmul(u, n1)));
+  }
+  __device__ __forceinline__ R ul() const {
+    return AXS ? xmul(sl(), vel(LI)) : xfma(w, l3, xfma(v, l2, xmul(u, l1)));
+  }
   __device__ __forceinline__ R um() const {
     if constexpr (AXS) return DIR == 2 ? -v : w;
-    return u * (n2 * l3 - n3 * l2) + v * (n3 * l1 - n1 * l3) + w * (n1 * l2 - n2 * l1);
+    return xfma(w, m3(), xfma(v, m2(), xmul(u, m1())));
   }
   // c = L f for one point (rows 0, 3, 4 through A = (V2,-u,-v,-w,1).f and
   // B = (un,-n).f: F0 - KK A and KK1 A +- X1 B)
   __device__ __forceinline__ void proj(R f0, R f1, R f2, R f3, R f4, R KK, R KK1, R X1, R V2_, R un_, R ul_,
                                        R um_, R* cc) const {
-    const R A = V2_ * f0 - u * f1 - v * f2 - w * f3 + f4;
-    cc[0] = f0 - KK * A;
+    const R A = xadd(xfma(-w, f3, xfma(-v, f2, xfma(-u, f1, xmul(V2_, f0)))), f4);
+    cc[0] = xfma(-KK, A, f0);
+    const R KA = xmul(KK1, A);
     if constexpr (AXS) {
       const R f[3] = {f1, f2, f3};
-      const R B = un_ * f0 - n1 * f[DIR];
-      cc[1] = sl() * f[LI] - ul_ * f0;
-      cc[2] = (DIR == 2 ? -f[MI] : f[MI]) - um_ * f0;
-      cc[3] = KK1 * A + X1 * B;
-      cc[4] = KK1 * A - X1 * B;
+      const R B = xfma(-n1, f[DIR], xmul(un_, f0));
+      cc[1] = xfma(-ul_, f0, xmul(sl(), f[LI]));
+      cc[2] = xfma(-um_, f0, DIR == 2 ? -f[MI] : f[MI]);
+      cc[3] = xfma(X1, B, KA);
+      cc[4] = xfma(-X1, B, KA);
     } else {
-      const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
-      const R B = un_ * f0 - n1 * f1 - n2 * f2 - n3 * f3;
-      cc[1] = l1 * f1 + l2 * f2 + l3 * f3 - ul_ * f0;
-      cc[2] = m1 * f1 + m2 * f2 + m3 * f3 - um_ * f0;
-      cc[3] = KK1 * A + X1 * B;
-      cc[4] = KK1 * A - X1 * B;
+      const R m1_ = m1(), m2_ = m2(), m3_ = m3();
+      const R B = xfma(-n3, f3, xfma(-n2, f2, xfma(-n1, f1, xmul(un_, f0))));
+      cc[1] = xfma(-ul_, f0, xfma(l3, f3, xfma(l2, f2, xmul(l1, f1))));
+      cc[2] = xfma(-um_, f0, xfma(m3_, f3, xfma(m2_, f2, xmul(m1_, f1))));
+      cc[3] = xfma(X1, B, KA);
+      cc[4] = xfma(-X1, B, KA);
     }
   }
   // hh = R h0 (OCFD_inviscous_character.f90:284-288), H = V2 + c^2/(gamma-1)
   __device__ __forceinline__ void back(const R* h0, R* hh, R inv_gm1) const {
     const R V2_ = V2(), un_ = un(), ul_ = ul(), um_ = um();
-    const R H = V2_ + c * c * inv_gm1;
-    hh[0] = h0[0] + h0[3] + h0[4];
+    const R H = xfma(xmul(c, c), inv_gm1, V2_);
+    hh[0] = xadd(xadd(h0[0], h0[3]), h0[4]);
     if constexpr (AXS) {
-      const R cs = c * n1;
+      const R cs = xmul(c, n1);
       R q[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         const R vk = vel(k);
         if (k == DIR)
-          q[k] = vk * h0[0] + (vk - cs) * h0[3] + (vk + cs) * h0[4];
+          q[k] = xfma(xadd(vk, cs), h0[4], xfma(xadd(vk, -cs), h0[3], xmul(vk, h0[0])));
         else if (k == LI)
-          q[k] = vk * h0[0] + sl() * h0[1] + vk * h0[3] + vk * h0[4];
+          q[k] = xfma(vk, h0[4], xfma(vk, h0[3], xfma(sl(), h0[1], xmul(vk, h0[0]))));
         else
-          q[k] = vk * h0[0] + (DIR == 2 ? -h0[2] : h0[2]) + vk * h0[3] + vk * h0[4];
+          q[k] = xfma(vk, h0[4], xfma(vk, h0[3], xadd(xmul(vk, h0[0]), DIR == 2 ? -h0[2] : h0[2])));
       }
       hh[1] = q[0];
       hh[2] = q[1];
       hh[3] = q[2];
     } else {
-      const R m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
-      hh[1] = u * h0[0] + l1 * h0[1] + m1 * h0[2] + (u - c * n1) * h0[3] + (u + c * n1) * h0[4];
-      hh[2] = v * h0[0] + l2 * h0[1] + m2 * h0[2] + (v - c * n2) * h0[3] + (v + c * n2) * h0[4];
-      hh[3] = w * h0[0] + l3 * h0[1] + m3 * h0[2] + (w - c * n3) * h0[3] + (w + c * n3) * h0[4];
+      const R m1_ = m1(), m2_ = m2(), m3_ = m3();
+      hh[1] = xfma(xfma(c, n1, u), h0[4],
+                   xfma(xfma(-c, n1, u), h0[3], xfma(m1_, h0[2], xfma(l1, h0[1], xmul(u, h0[0])))));
+      hh[2] = xfma(xfma(c, n2, v), h0[4],
+                   xfma(xfma(-c, n2, v), h0[3], xfma(m2_, h0[2], xfma(l2, h0[1], xmul(v, h0[0])))));
+      hh[3] = xfma(xfma(c, n3, w), h0[4],
+                   xfma(xfma(-c, n3, w), h0[3], xfma(m3_, h0[2], xfma(l3, h0[1], xmul(w, h0[0])))));
     }
-    hh[4] = V2_ * h0[0] + ul_ * h0[1] + um_ * h0[2] + (H - c * un_) * h0[3] + (H + c * un_) * h0[4];
+    hh[4] = xfma(xfma(c, un_, H), h0[4],
+                 xfma(xfma(-c, un_, H), h0[3], xfma(um_, h0[2], xfma(ul_, h0[1], xmul(V2_, h0[0])))));
   }
 };
 
@@ -799,22 +812,23 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         }
       } else {
         // face state: arithmetic means of the two neighbours (:205-211)
-        const R u1 = (W(10, 3) + W(10, 4)) * R(0.5);
-        const R v1 = (W(11, 3) + W(11, 4)) * R(0.5);
-        const R w1 = (W(12, 3) + W(12, 4)) * R(0.5);
-        const R c1 = (W(13, 3) + W(13, 4)) * R(0.5);
-        const R a1 = (AXS && DIR != 0) ? R(0) : (W(14, 3) + W(14, 4)) * R(0.5);
-        const R a2 = (AXS && DIR != 1) ? R(0) : (W(15, 3) + W(15, 4)) * R(0.5);
-        const R a3 = (AXS && DIR != 2) ? R(0) : (W(16, 3) + W(16, 4)) * R(0.5);
+        auto mean = [&](int var) -> R { return xmul(xadd(W(var, 3), W(var, 4)), R(0.5)); };
+        const R u1 = mean(10);
+        const R v1 = mean(11);
+        const R w1 = mean(12);
+        const R c1 = mean(13);
+        const R a1 = (AXS && DIR != 0) ? R(0) : mean(14);
+        const R a2 = (AXS && DIR != 1) ? R(0) : mean(15);
+        const R a3 = (AXS && DIR != 2) ? R(0) : mean(16);
         // orthonormal basis (n,l,m) and L = S, R = S^-1 (:216-248)
 #if OCFD_FEWER_DIVS
         CharBasis<DIR, AXS, R> cb;
         cb.init(u1, v1, w1, c1, a1, a2, a3);
         const R V2 = cb.V2(), un = cb.un(), ul = cb.ul(), um = cb.um();
         const R rc = R(1) / c1;
-        const R KK = (R(ph.gamma) - R(1)) * (rc * rc);
-        const R KK1 = KK * R(0.5);
-        const R X1 = R(0.5) * rc;
+        const R KK = xmul(xadd(R(ph.gamma), R(-1)), xmul(rc, rc));
+        const R KK1 = xmul(KK, R(0.5));
+        const R X1 = xmul(R(0.5), rc);
         // rows of L through two shared dot products: with A = (V2,-u,-v,-w,1).F and
         // B = (un,-n1,-n2,-n3,0).F, rows 0, 3, 4 are F0 - KK A and KK1 A +- X1 B
         auto proj5v = [&](R f0, R f1, R f2, R f3, R f4, R* c) {
@@ -883,21 +897,21 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               R f4[4];
               W4(0, 7, f4);
 #pragma unroll
-              for (int v = 0; v < 4; v++) G[v] = oa[0] * f4[v];
-              G[4] = oa[0] * W(4, 7);
+              for (int v = 0; v < 4; v++) G[v] = xmul(oa[0], f4[v]);
+              G[4] = xmul(oa[0], W(4, 7));
 #pragma unroll
               for (int q = 6; q >= 0; q--) {
                 W4(0, q, f4);
 #pragma unroll
-                for (int v = 0; v < 4; v++) G[v] = G[v] + oa[7 - q] * f4[v];
-                G[4] = G[4] + oa[7 - q] * W(4, q);
+                for (int v = 0; v < 4; v++) G[v] = xfma(oa[7 - q], f4[v], G[v]);
+                G[4] = xfma(oa[7 - q], W(4, q), G[4]);
               }
             } else {
 #pragma unroll
               for (int v = 0; v < 5; v++) {
-                R acc = oa[0] * W(v, 7);
+                R acc = xmul(oa[0], W(v, 7));
 #pragma unroll
-                for (int q = 6; q >= 0; q--) acc = acc + oa[7 - q] * W(v, q);
+                for (int q = 6; q >= 0; q--) acc = xfma(oa[7 - q], W(v, q), acc);
                 G[v] = acc;
               }
             }
@@ -908,8 +922,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             proj5(0, 4, pc);
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              const R mp = pb[r] + minmod2((pc[r] - pb[r]), kap * (pb[r] - pa[r]));
-              dfl |= ((dP[r] - pb[r]) * (dP[r] - mp) >= ep ? 1u : 0u) << r;
+              const R mp = xadd(pb[r], minmod2(xadd(pc[r], -pb[r]), xmul(kap, xadd(pb[r], -pa[r]))));
+              dfl |= (xmul(xadd(dP[r], -pb[r]), xadd(dP[r], -mp)) >= ep ? 1u : 0u) << r;
             }
           }
           {
@@ -919,21 +933,21 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               R f4[4];
               W4(5, 0, f4);
 #pragma unroll
-              for (int v = 0; v < 4; v++) G[v] = oa[0] * f4[v];
-              G[4] = oa[0] * W(9, 0);
+              for (int v = 0; v < 4; v++) G[v] = xmul(oa[0], f4[v]);
+              G[4] = xmul(oa[0], W(9, 0));
 #pragma unroll
               for (int q = 1; q <= 7; q++) {
                 W4(5, q, f4);
 #pragma unroll
-                for (int v = 0; v < 4; v++) G[v] = G[v] + oa[q] * f4[v];
-                G[4] = G[4] + oa[q] * W(9, q);
+                for (int v = 0; v < 4; v++) G[v] = xfma(oa[q], f4[v], G[v]);
+                G[4] = xfma(oa[q], W(9, q), G[4]);
               }
             } else {
 #pragma unroll
               for (int v = 0; v < 5; v++) {
-                R acc = oa[0] * W(5 + v, 0);
+                R acc = xmul(oa[0], W(5 + v, 0));
 #pragma unroll
-                for (int q = 1; q <= 7; q++) acc = acc + oa[q] * W(5 + v, q);
+                for (int q = 1; q <= 7; q++) acc = xfma(oa[q], W(5 + v, q), acc);
                 G[v] = acc;
               }
             }
@@ -944,8 +958,8 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             proj5(5, 5, pc);
 #pragma unroll
             for (int r = 0; r < 5; r++) {
-              const R mp = pb[r] + minmod2((pa[r] - pb[r]), kap * (pb[r] - pc[r]));
-              dfl |= ((dM[r] - pb[r]) * (dM[r] - mp) >= ep ? 1u : 0u) << (5 + r);
+              const R mp = xadd(pb[r], minmod2(xadd(pa[r], -pb[r]), xmul(kap, xadd(pb[r], -pc[r]))));
+              dfl |= (xmul(xadd(dM[r], -pb[r]), xadd(dM[r], -mp)) >= ep ? 1u : 0u) << (5 + r);
             }
           }
           if (dfl) {
@@ -1118,7 +1132,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       // back to physical space, hh = R h0 (OCFD_inviscous_character.f90:284-288)
       R h0[5];
 #pragma unroll
-      for (int r = 0; r < 5; r++) h0[r] = dP[r] + dM[r];
+      for (int r = 0; r < 5; r++) h0[r] = xadd(dP[r], dM[r]);
       R hh[5];
       dcb.back(h0, hh, R(ph.inv_gm1));
 #pragma unroll
@@ -1201,9 +1215,11 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_face_batch(BatchTab<Fac
         A, bx, by, bz, reinterpret_cast<R*>(smem_raw));
 }
 
-// Single-instance sweep of a periodic direction with the input tiles staged by
-// TMA (the arithmetic is that of k_face).
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false>
+// Single-instance sweep with the input tiles staged by TMA (the arithmetic is
+// that of k_face).  ALLIN: a periodic direction; otherwise the sweep includes
+// the boundary closures, and tile points past the haloed array (read as zeros
+// by the copy) are not used.
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false, bool ALLIN = true>
 __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant__ FaceTmaMaps tm) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
@@ -1255,7 +1271,7 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
     }
     return;
   }
-  face_body<DIR, CHAR, SCHEME, true, NP, TF, R, S, true, AXS>(a, bx, by, bz, sm, tile, toff, qbase);
+  face_body<DIR, CHAR, SCHEME, ALLIN, NP, TF, R, S, true, AXS>(a, bx, by, bz, sm, tile, toff, qbase);
 }
 
 
@@ -1323,12 +1339,12 @@ inline bool tma_strides_ok(const Grid& g) {
   return ((long long)g.nxh * sizeof(S)) % 16 == 0 && ((long long)g.nxh * g.nyh * sizeof(S)) % 16 == 0;
 }
 
-template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false>
+template <int DIR, bool CHAR, int SCHEME, typename R, typename S, bool AXS = false, bool ALLIN = true>
 static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
   constexpr int NP = FaceTile<DIR, CHAR, SCHEME>::NP, TF = FaceTile<DIR, CHAR, SCHEME>::TF;
   using B = TmaBox<DIR, NP, TF, S>;
   constexpr size_t smem = FaceTmaSmem<DIR, CHAR, SCHEME, NP, TF, R, S>::BYTES;
-  auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S, AXS>;
+  auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S, AXS, ALLIN>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   FaceTmaMaps tm;
   const S* arr[8] = {a.d, a.u, a.v, a.w, a.T, a.A1, a.A2, a.A3};
@@ -1339,7 +1355,7 @@ static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
 }
 
 // One (direction, form, scheme) combination: the TMA-staged sweep for FP64
-// periodic directions (measured 1-3% faster at 256^3; the FP32 sweeps, four
+// (periodic directions measured 1-3% faster at 256^3; the FP32 sweeps, four
 // blocks per SM, are as fast or faster with plain loads), the axis-aligned
 // variant when the metric row allows it (production build).  An empty grid
 // asks for the shared-memory attribute of every variant instead.
@@ -1353,15 +1369,21 @@ static cudaError_t launch_face_dc(const FaceArgs<S>& a, cudaStream_t st) {
     if constexpr (sizeof(S) == 8) {
       if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S>(a, st);
       if (kAx && e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, kAx>(a, st);
+      if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
     }
     return e;
   }
   const bool allin = a.ph.periodic[D] != 0;
-  if (!allin) return launch_face_t<D, C, SC, false, R, S>(a, st);
+  const bool tma = sizeof(S) == 8 && !a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g);
+  if (!allin) {
+    if constexpr (sizeof(S) == 8) {
+      if (tma) return launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
+    }
+    return launch_face_t<D, C, SC, false, R, S>(a, st);
+  }
   const bool ax = kAx && axis_aligned<D>(a.ph.metzero);
   if constexpr (sizeof(S) == 8) {
-    if (!a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g))
-      return ax ? launch_face_tma_t<D, C, SC, R, S, kAx>(a, st) : launch_face_tma_t<D, C, SC, R, S>(a, st);
+    if (tma) return ax ? launch_face_tma_t<D, C, SC, R, S, kAx>(a, st) : launch_face_tma_t<D, C, SC, R, S>(a, st);
   }
   return ax ? launch_face_t<D, C, SC, true, R, S, kAx>(a, st) : launch_face_t<D, C, SC, true, R, S>(a, st);
 }

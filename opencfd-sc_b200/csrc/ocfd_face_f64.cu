@@ -24,7 +24,7 @@ static TileEncodeFn tile_encoder() {
   return fn;
 }
 
-// TMA staging of the periodic face sweeps: on unless OCFD_FACE_TMA=0 (or the
+// TMA staging of the FP64 face sweeps: on unless OCFD_FACE_TMA=0 (or the
 // driver offers no tensor-map encoder).
 bool face_tma_enabled() {
   static int on = -1;

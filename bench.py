@@ -597,6 +597,9 @@ def run_serve(args):
     srv = serving.Server(mixed=True, round_steps=args.round_steps, keep=sample)
     served = srv.run(reqs, realtime=True, payloads=payloads)
     seq = serving.run_sequential(reqs, mixed=False, keep=sample, payloads=payloads)
+    # the same requests solved one after another in mixed precision: the served
+    # stream against it is the gain of batching alone
+    seq_m = serving.run_sequential(reqs, mixed=True, payloads=payloads)
 
     inner = (slice(4, -4),) * 3
 
@@ -624,15 +627,35 @@ def run_serve(args):
         s.close()
     agg = lambda L: {f"{k}_rel_max": max(e[k] for e in L) for k in ("ke", "rho", "u", "p")} | {
         f"{k}_rel_median": float(np.median([e[k] for e in L])) for k in ("ke", "u")}
+    # per request at a short horizon (before the chaotic growth of rounding
+    # differences): mixed against FP64 after HS steps, both alone -- a served
+    # result is bit-identical to the same request solved alone
+    HS = 20
+    short = []
+    for rid in sample:
+        p, xyz, prims = payloads[rid]
+        out = []
+        for prec in (1, 0):
+            q = p.copy()
+            q.precision = prec
+            s = serving._start(q, xyz, prims, 0)
+            s.step(HS)
+            out.append((s.download_state(), s.show_flow_msg().tolist()))
+            s.close()
+        short.append(errors(out[0][0], out[0][1], out[1][0], out[1][1], reqs[rid].ma))
     work = sum(r.n ** 3 * r.steps for r in reqs)
     line = {
         "metric": "served stream: aggregate GPts/s and p50/p99 time-to-result, mixed precision, continuous batching",
         "mode": "serve", "requests": len(reqs), "rate_per_s": args.rate, "work_gpt_steps": work,
         "data": "synthetic (seeded Poisson stream of TGV / isotropic-turbulence requests, sizes 32^3-128^3)",
         "served_mixed": {k: served[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s", "rounds", "batched_rounds",
+                                                 "persistent_rounds",
                                                  "max_active")},
         "sequential_fp64": {k: seq[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s", "wall_s")},
+        "sequential_mixed": {k: seq_m[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s", "wall_s")},
         "throughput_ratio": served["gpts_per_s"] / seq["gpts_per_s"],
+        "throughput_ratio_vs_sequential_mixed": served["gpts_per_s"] / seq_m["gpts_per_s"],
+        "error_vs_fp64_at_20_steps": {"sample": len(sample), **agg(short)},
         "error_vs_fp64": {"sample": len(sample), **agg(mixed_err)},
         "fp64_perturbed_2^-24_vs_fp64": agg(floor_err),
         "scheme": "WENO7 flux-vector, SW, CD6; dt at CFL 0.5 from the initial field",

@@ -373,8 +373,13 @@ int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f, const doub
  * per kernel and per RK stage for the whole batch (18 launches, ragged grids
  * in the same launch), captured as a CUDA graph; the face-sweep tile shape per
  * direction is chosen by timing the candidates on the first step
- * (autotuning).  Otherwise the members advance concurrently on their own
- * streams.  Results are bit-identical to stepping each member alone.
+ * (autotuning).  For the flux-vector WENO7 and the characteristic OMP6 forms
+ * (viscous) a stage is instead ONE persistent launch for the whole batch
+ * (3 launches per step): resident blocks take the tiles of every member's face
+ * sweeps, viscous gradients, stage tail and negative-T repair from one work
+ * list, a member's tail starting as soon as its own fluxes are complete.
+ * Otherwise the members advance concurrently on their own streams.  Results
+ * are bit-identical to stepping each member alone.
  * Between batch steps a member may be used on its own (downloads,
  * diagnostics, single steps); the batch rebuilds its tables when needed.
  * ------------------------------------------------------------------------- */
@@ -388,6 +393,22 @@ int ocfd_batch_set_tiles(ocfd_batch* b, const int variants[3]);
 /* *fused = 1 when the batch runs one launch per kernel for all members;
  * variants[3] = the tile variants in use (after the first step). */
 int ocfd_batch_info(const ocfd_batch* b, int* fused, int variants[3]);
+/* Launch mode where the persistent stage kernel exists: on = -1 (the
+ * default) times two steps in each mode at the first batch step of at least
+ * four steps and keeps the faster (those steps are real steps: both modes give
+ * the same bits); 0: one launch per kernel and stage; 1: the persistent
+ * kernel. */
+int ocfd_batch_set_persistent(ocfd_batch* b, int on);
+/* 0: members advance on their own graphs; 1: one batched launch per kernel
+ * and stage; 2: one persistent launch per stage.  OCFD_E_TIMEOUT from a batch
+ * step (sync = 1) or from a member's ocfd_gpu_sync after mode 2: a bounded
+ * dependency wait inside the persistent kernel gave up (about a second); the
+ * steps since the last synchronisation are invalid and the batch continues in
+ * mode 1. */
+int ocfd_batch_mode(const ocfd_batch* b);
+/* ms[0], ms[1]: device time of the two steps timed in mode 1 and in mode 2 by
+ * the launch-mode choice; OCFD_E_STATE before that choice was timed. */
+int ocfd_batch_mode_times(const ocfd_batch* b, float ms[2]);
 const char* ocfd_batch_last_error(const ocfd_batch* b);
 void ocfd_batch_destroy(ocfd_batch* b);
 

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -42,6 +43,7 @@ struct ocfd_handle {
   void* ev = nullptr;
   double* scratch = nullptr;
   size_t scratch_n = 0;
+  void* slab = nullptr;  // the arrays of ocfd_gpu_create, one stream-ordered block
   DevStatus* dstat = nullptr;
   DevStatus* hstat = nullptr;  // pinned
   double* dout = nullptr;      // small device output block
@@ -192,6 +194,34 @@ size_t rsize() {
   return sizeof(R);
 }
 
+// The device memory pool of the instances on one device (created on first use):
+// an instance's arrays are one block allocated and freed in stream order on the
+// instance's stream, so that creating and destroying instances (the serving
+// loop admits and retires them while others run) never synchronises the device
+// as cudaMalloc / cudaFree do.  Freed blocks stay in the pool for the next
+// instance (release threshold: never) while any instance lives on the device;
+// when the last one is destroyed the pool returns its memory to the device.
+std::mutex pool_mu;
+cudaMemPool_t pools[64] = {};
+int pool_live[64] = {};
+cudaMemPool_t instance_pool(int device) {
+  if (device < 0 || device >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(pool_mu);
+  if (!pools[device]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = pool;
+  }
+  return pools[device];
+}
+
 }  // namespace
 
 // =====================================================================================
@@ -314,6 +344,13 @@ int ocfd_gpu_sync(ocfd_handle* h) {
                 "a bounded device wait gave up (tile copy): the results of the steps since the last "
                 "synchronisation are invalid; this handle no longer uses TMA tile staging");
   }
+  if (h->hstat->error == 5) {
+    CK(cudaMemsetAsync(&h->dstat->error, 0, sizeof(int), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return fail(h, OCFD_E_TIMEOUT,
+                "a bounded device wait of the persistent batched stage kernel gave up: the results of the "
+                "steps since the last synchronisation are invalid");
+  }
   return OCFD_OK;
 }
 
@@ -326,26 +363,16 @@ void ocfd_gpu_destroy(ocfd_handle* h) {
   auto F = [](void* p) {
     if (p) cudaFree(p);
   };
-  F(h->f);
-  F(h->fn);
-  F(h->du);
-  for (int q = 0; q < 5; q++) {
-    F(h->prim[q]);
-    F(h->p32[q]);
+  // the instance's arrays return to the library's pool in stream order (no
+  // device-wide synchronisation, unlike cudaFree)
+  if (h->slab) {
+    cudaFreeAsync(h->slab, h->st);
+    std::lock_guard<std::mutex> lk(pool_mu);
+    if (--pool_live[h->device] == 0 && pools[h->device]) {
+      cudaStreamSynchronize(h->st);
+      cudaMemPoolTrimTo(pools[h->device], 0);
+    }
   }
-  F(h->q32);
-  F(h->talt);
-  for (int m = 0; m < OCFD_N_METRICS; m++) {
-    F(h->met[m]);
-    F(h->met32[m]);
-  }
-  F(h->rh);
-  for (int q = 0; q < 3; q++) F(h->hf[q]);
-  F(h->ev);
-  F(h->scratch);
-  F(h->dstat);
-  F(h->dout);
-  F(h->dptr);
   F(h->bl_inlet);
   F(h->bl_upper);
   F(h->bl_pertb);
@@ -386,10 +413,14 @@ int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
   const Grid& g = h->g;
   const size_t n = (size_t)g.n, nh = (size_t)g.nh;
   const size_t r = h->mixed ? 4 : 8;
+  // every array in one block from the library's per-device pool: the layout
+  // first (256-byte aligned offsets), then one stream-ordered allocation
+  std::vector<std::pair<void**, size_t>> lay;
+  size_t total = 0;
 #define AL(ptr, bytes)                                       \
   do {                                                       \
-    e = cudaMalloc((void**)&(ptr), (bytes));                 \
-    if (e != cudaSuccess) { ocfd_gpu_destroy(h); return OCFD_E_NOMEM; } \
+    lay.push_back({(void**)&(ptr), total});                  \
+    total += ((size_t)(bytes) + 255) & ~(size_t)255;         \
   } while (0)
   AL(h->f, 5 * n * 8);
   AL(h->fn, 5 * n * 8);
@@ -414,6 +445,19 @@ int ocfd_gpu_create(const ocfd_params* pin, int device, ocfd_handle** out) {
   AL(h->dout, 64 * 8);
   AL(h->dptr, 64 * sizeof(double*));
 #undef AL
+  cudaMemPool_t pool = instance_pool(device);
+  if (!pool) return bad(cudaErrorMemoryAllocation, "instance memory pool");
+  e = cudaMallocFromPoolAsync(&h->slab, total, pool, h->st);
+  if (e != cudaSuccess) {
+    h->slab = nullptr;
+    ocfd_gpu_destroy(h);
+    return OCFD_E_NOMEM;
+  }
+  {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    pool_live[device]++;
+  }
+  for (auto& it : lay) *it.first = (char*)h->slab + it.second;
   e = cudaMallocHost((void**)&h->hstat, sizeof(DevStatus));
   if (e != cudaSuccess) return bad(e, "cudaMallocHost");
   e = cudaMallocHost((void**)&h->hout, 64 * 8);
@@ -1009,6 +1053,7 @@ static int fused_stage(ocfd_handle* h, int krk, Prof* pf = nullptr) {
   }
   prof_mark(h, pf, 6);
   UpdArgs<double> fx = upd_args<double>(h);
+  fx.krk = krk;  // lean stages 1-2: the repair recovers d,u,v,w from f
   CK(launch_negt_fix(fx, h->st));
   swap_t(h);
   if (!h->fuse_bc) {
@@ -1308,15 +1353,25 @@ struct ocfd_batch {
   int variant[3] = {0, 0, 0};   // face tile variant per direction
   int forced[3] = {-1, -1, -1};
   bool tuned = false;
-  // per parity: device tables and the captured step
+  // per launch mode (0: one launch per kernel and stage, 1: one persistent
+  // launch per stage) and parity: device tables and the captured step
   struct Par {
     void* dev = nullptr;
     size_t bytes = 0;
     cudaGraphExec_t graph = nullptr;
-  } par[2];
+  } par[2][2];
   std::vector<double*> f0, t0;  // members' f and T at table build (parity 0)
   std::vector<int> mver;        // members' metric versions at table build
   int nblk_face[3] = {0, 0, 0}, nblk_upd = 0;
+  // persistent stage kernel: one launch per RK stage (mode 2)
+  int pmode = -1;             // ocfd_batch_set_persistent: -1 timed choice, 0 off, 1 on
+  bool persist = false;       // the steps use it (the launch mode in use)
+  bool have_p = false;        // persistent graphs captured
+  bool mode_tuned = false;    // launch mode chosen (by timing, or forced)
+  float tmode[2] = {0.f, 0.f};  // measured ms of two steps per launch mode
+  int vstage = 0;             // its face tile variant (one for the three directions)
+  int per_sm = 0, nsm = 0;    // its resident blocks per SM, the device's SMs
+  float tvar[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // autotune: face time per direction and variant
   std::string err;
 };
 
@@ -1342,6 +1397,18 @@ bool batch_fusable(const std::vector<ocfd_handle*>& m) {
         (h->p.if_viscous != 0) != (a->p.if_viscous != 0))
       return false;
   }
+  return true;
+}
+
+// Whether the batch runs one persistent launch per stage: a kernel exists for
+// its combination, it is allowed, and forced tile variants (if any) agree in
+// the three directions.
+bool batch_persistent(const ocfd_batch* b) {
+  const ocfd_handle* h = b->m[0];
+  if (!b->fused || b->pmode == 0) return false;
+  if (!batch_stage_supported(h->chr, h->p.scheme_invis, h->p.if_viscous != 0)) return false;
+  for (int d = 1; d < 3; d++)
+    if (b->forced[d] != b->forced[0]) return false;
   return true;
 }
 
@@ -1379,7 +1446,7 @@ void block_ranges(const std::vector<dim3>& dims, std::vector<int4>& ent, int& to
 // buffer pointers are advanced through the step exactly as fused_step does and
 // restored afterwards.
 template <typename R>
-static int batch_capture(ocfd_batch* b, int parity) {
+static int batch_capture(ocfd_batch* b, int parity, bool persist) {
   typedef R S;
   std::vector<ocfd_handle*>& M = b->m;
   const int n = (int)M.size();
@@ -1437,14 +1504,52 @@ static int batch_capture(ocfd_batch* b, int parity) {
       ua[q].krk = krk;
       ua[q].du = nullptr;
       na[q] = upd_args<double>(M[q]);
+      na[q].krk = krk;
     }
     o.upd = im.put(ua.data(), n * sizeof(UpdArgs<R>));
     o.negt = im.put(na.data(), n * sizeof(UpdArgs<double>));
     for (ocfd_handle* h : M) swap_t(h);
   }
   restore();
+  // persistent stage kernel: the work list (the same for the three stages) and
+  // per stage a zeroed counter block
+  size_t o_seg = 0, o_need = 0, o_ctr = 0;
+  int nseg = 0, nitems = 0;
+  const size_t ctr_ints = 1 + 2 * (size_t)n;
+  if (persist) {
+    std::vector<int4> seg;
+    std::vector<int2> need(n);
+    auto add = [&](int q, int kind, dim3 g) {
+      const int cnt = (int)(g.x * g.y * g.z);
+      if (cnt == 0) return 0;
+      seg.push_back(make_int4(nitems, q * 8 + kind, (int)g.x, (int)g.y));
+      nitems += cnt;
+      return cnt;
+    };
+    auto phase_a = [&](int q) {
+      int c = 0;
+      for (int d = 0; d < 3; d++) c += add(q, BW_FACE_X + d, face_batch_dims<S>(d, b->vstage, face_args<S>(M[q], d)));
+      if (h0->p.if_viscous) c += add(q, BW_VISC, update_dims(M[q]->g));
+      need[q].x = c;
+    };
+    auto tail = [&](int q) { need[q].y = add(q, BW_TAIL, update_dims(M[q]->g)); };
+    // A0 A1 T0 A2 T1 ... A(n-1) T(n-2) T(n-1), then the repairs: everything an
+    // item waits for is listed before it
+    phase_a(0);
+    for (int q = 1; q < n; q++) {
+      phase_a(q);
+      tail(q - 1);
+    }
+    tail(n - 1);
+    for (int q = 0; q < n; q++) add(q, BW_NEGT, dim3(1, 1, 1));
+    nseg = (int)seg.size();
+    o_seg = im.put(seg.data(), seg.size() * sizeof(int4));
+    o_need = im.put(need.data(), n * sizeof(int2));
+    std::vector<int> zero(3 * ctr_ints, 0);
+    o_ctr = im.put(zero.data(), zero.size() * sizeof(int));
+  }
   // upload
-  ocfd_batch::Par& P = b->par[parity];
+  ocfd_batch::Par& P = b->par[persist ? 1 : 0][parity];
   if (P.graph) {
     cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
@@ -1467,6 +1572,13 @@ static int batch_capture(ocfd_batch* b, int parity) {
   // capture: per stage the sensor (per member), 3 face sweeps, the viscous
   // gradients, the tail and the repair, all on the batch stream
   const bool hybrid = h0->p.scheme_invis == OCFD_SCHEME_HYBRID;
+  // FP32 tails: 32-bit face and viscous-flux offsets when every member's fit
+  bool i32 = sizeof(R) == 4;
+  for (const ocfd_handle* h : M) {
+    long long fmax = 0;
+    for (int d = 0; d < 3; d++) fmax = std::max(fmax, h->fs[d]);
+    i32 = i32 && 12LL * h->g.n < 2147483647LL && 10LL * fmax < 2147483647LL;
+  }
   std::vector<cudaStream_t> own(n);
   for (int q = 0; q < n; q++) own[q] = M[q]->st;
   cudaGraph_t graph;
@@ -1487,6 +1599,24 @@ static int batch_capture(ocfd_batch* b, int parity) {
         r = ocfd_gpu_rhybrid(M[q]);
         M[q]->st = own[q];
       }
+    if (persist) {
+      if (krk == 1 && e == cudaSuccess) e = cudaMemsetAsync(base + o_ctr, 0, 3 * ctr_ints * sizeof(int), b->st);
+      StageTab<R> t;
+      for (int d = 0; d < 3; d++) t.face[d] = (const FaceArgs<R>*)(base + o.face[d]);
+      t.visc = (const ViscArgs<R, R>*)(base + o.visc);
+      t.upd = (const UpdArgs<R>*)(base + o.upd);
+      t.negt = (const UpdArgs<double>*)(base + o.negt);
+      t.seg = (const int4*)(base + o_seg);
+      t.need = (const int2*)(base + o_need);
+      t.ctr = (int*)(base + o_ctr) + (krk - 1) * ctr_ints;
+      t.nseg = nseg;
+      t.nitems = nitems;
+      t.count = n;
+      const int grid = std::max(1, std::min(nitems, b->nsm * b->per_sm));
+      if (e == cudaSuccess) e = launch_batch_stage<R>(h0->chr, h0->p.scheme_invis, b->vstage, t, grid, b->st, nullptr);
+      for (ocfd_handle* h : M) swap_t(h);
+      continue;
+    }
     for (int d = 0; d < 3 && e == cudaSuccess; d++) {
       auto t = tab(o.face[d], o_ent_face[d]);
       BatchTab<FaceArgs<S>> bt = {(const FaceArgs<S>*)t.a, t.e, n};
@@ -1500,7 +1630,7 @@ static int batch_capture(ocfd_batch* b, int parity) {
     if (e == cudaSuccess) {
       auto t = tab(o.upd, o_ent_upd);
       BatchTab<UpdArgs<R>> bt = {(const UpdArgs<R>*)t.a, t.e, n};
-      e = launch_fused_batch<R>(bt, b->nblk_upd, h0->chr, h0->p.if_viscous != 0, true, b->st);
+      e = launch_fused_batch<R>(bt, b->nblk_upd, h0->chr, h0->p.if_viscous != 0, true, i32, b->st);
     }
     if (e == cudaSuccess) {
       auto t = tab(o.negt, o_ent_upd);
@@ -1572,6 +1702,7 @@ static int batch_autotune(ocfd_batch* b) {
         cudaEventElapsedTime(&ms, e0, e1);
         if (rep > 0) tot += ms;  // first launch is a warm-up
       }
+      b->tvar[d][v] = tot;
       if (tot < best) {
         best = tot;
         b->variant[d] = v;
@@ -1590,10 +1721,11 @@ static int batch_autotune(ocfd_batch* b) {
 static int batch_prepare(ocfd_batch* b) {
   BCK(cudaStreamSynchronize(b->st));  // no launch in flight reads the old tables
   for (int P = 0; P < 2; P++)
-    if (b->par[P].graph) {
-      cudaGraphExecDestroy(b->par[P].graph);
-      b->par[P].graph = nullptr;
-    }
+    for (int M = 0; M < 2; M++)
+      if (b->par[M][P].graph) {
+        cudaGraphExecDestroy(b->par[M][P].graph);
+        b->par[M][P].graph = nullptr;
+      }
   const bool mixed = b->m[0]->mixed;
   int r = OCFD_OK;
   if (!b->tuned) {
@@ -1601,7 +1733,37 @@ static int batch_prepare(ocfd_batch* b) {
     if (r) return r;
     b->tuned = true;
   }
-  for (int P = 0; P < 2 && r == OCFD_OK; P++) r = mixed ? batch_capture<float>(b, P) : batch_capture<double>(b, P);
+  b->have_p = batch_persistent(b);
+  if (b->have_p) {
+    // one tile variant for the three sweeps of the persistent kernel: the
+    // forced one, else the one with the shorter total face time
+    const ocfd_handle* h = b->m[0];
+    b->vstage = b->forced[0] >= 0 ? b->forced[0]
+                                  : (b->tvar[0][1] + b->tvar[1][1] + b->tvar[2][1] <
+                                             b->tvar[0][0] + b->tvar[1][0] + b->tvar[2][0]
+                                         ? 1
+                                         : 0);
+    StageTab<double> t64;
+    StageTab<float> t32;
+    memset(&t64, 0, sizeof(t64));
+    memset(&t32, 0, sizeof(t32));
+    cudaError_t e = mixed ? launch_batch_stage<float>(h->chr, h->p.scheme_invis, b->vstage, t32, 0, b->st, &b->per_sm)
+                          : launch_batch_stage<double>(h->chr, h->p.scheme_invis, b->vstage, t64, 0, b->st, &b->per_sm);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
+    if (e != cudaSuccess) return bfail(b, OCFD_E_CUDA, std::string("persistent stage kernel set-up: ") + cudaGetErrorString(e));
+    if (b->per_sm < 1) b->have_p = false;  // does not fit on an SM: one launch per kernel instead
+  }
+  // the launch mode to capture: the chosen one, or one launch per kernel while
+  // the choice is open (the persistent graphs are captured when it is timed)
+  if (!b->have_p) {
+    b->persist = false;
+    b->mode_tuned = true;
+  } else if (b->pmode == 1) {
+    b->persist = true;
+    b->mode_tuned = true;
+  }
+  for (int P = 0; P < 2 && r == OCFD_OK; P++)
+    r = mixed ? batch_capture<float>(b, P, b->persist) : batch_capture<double>(b, P, b->persist);
   if (r) return r;
   b->f0.clear();
   b->t0.clear();
@@ -1657,8 +1819,32 @@ int ocfd_batch_info(const ocfd_batch* b, int* fused, int variants[3]) {
   if (!b) return OCFD_E_PARAM;
   if (fused) *fused = b->fused ? 1 : 0;
   if (variants)
-    for (int d = 0; d < 3; d++) variants[d] = b->variant[d];
+    for (int d = 0; d < 3; d++) variants[d] = b->persist ? b->vstage : b->variant[d];
   return OCFD_OK;
+}
+
+int ocfd_batch_set_persistent(ocfd_batch* b, int on) {
+  if (!b || on < -1 || on > 1) return OCFD_E_PARAM;
+  b->pmode = on;
+  b->mode_tuned = false;
+  b->persist = false;
+  b->f0.clear();  // rebuild at the next step
+  return OCFD_OK;
+}
+
+int ocfd_batch_mode(const ocfd_batch* b) {
+  if (!b) return OCFD_E_PARAM;
+  if (!b->fused) return 0;
+  if (!batch_persistent(b)) return 1;
+  if (b->pmode == 1) return 2;
+  return b->mode_tuned && b->persist ? 2 : 1;
+}
+
+int ocfd_batch_mode_times(const ocfd_batch* b, float ms[2]) {
+  if (!b || !ms) return OCFD_E_PARAM;
+  ms[0] = b->tmode[0];
+  ms[1] = b->tmode[1];
+  return b->mode_tuned && b->tmode[0] > 0.f ? OCFD_OK : OCFD_E_STATE;
 }
 
 const char* ocfd_batch_last_error(const ocfd_batch* b) { return b ? b->err.c_str() : "null batch"; }
@@ -1706,7 +1892,46 @@ int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
       if (r) return r;
       par = 0;
     }
-    BCK(cudaGraphLaunch(b->par[par].graph, b->st));
+    if (!b->mode_tuned && nsteps - s >= 4 && par == 0) {
+      // launch-mode choice: two steps (both parities) in each mode, timed on
+      // the stream; the steps are real steps (both modes give the same bits)
+      BCK(cudaStreamSynchronize(b->st));  // the tables of the capture below are not in use
+      const bool mixed = b->m[0]->mixed;
+      for (int P = 0; P < 2; P++) {
+        int r = mixed ? batch_capture<float>(b, P, true) : batch_capture<double>(b, P, true);
+        if (r) return r;
+      }
+      cudaEvent_t ev[3];
+      for (int q = 0; q < 3; q++) BCK(cudaEventCreate(&ev[q]));
+      BCK(cudaEventRecord(ev[0], b->st));
+      for (int q = 0; q < 4; q++) {
+        const int M = q < 2 ? 0 : 1;
+        BCK(cudaGraphLaunch(b->par[M][par].graph, b->st));
+        for (ocfd_handle* h : b->m) {
+          std::swap(h->f, h->fn);
+          std::swap(h->prim[4], h->talt);
+          h->istep += 1;
+          h->tt += h->p.dt;
+        }
+        par ^= 1;
+        if (q == 1) BCK(cudaEventRecord(ev[1], b->st));
+      }
+      BCK(cudaEventRecord(ev[2], b->st));
+      BCK(cudaEventSynchronize(ev[2]));
+      cudaEventElapsedTime(&b->tmode[0], ev[0], ev[1]);
+      cudaEventElapsedTime(&b->tmode[1], ev[1], ev[2]);
+      for (int q = 0; q < 3; q++) cudaEventDestroy(ev[q]);
+      b->persist = b->tmode[1] < b->tmode[0];
+      b->mode_tuned = true;
+      for (int P = 0; P < 2; P++) {  // the other mode's graphs are not used again
+        ocfd_batch::Par& X = b->par[b->persist ? 0 : 1][P];
+        if (X.graph) cudaGraphExecDestroy(X.graph);
+        X.graph = nullptr;
+      }
+      s += 3;
+      continue;
+    }
+    BCK(cudaGraphLaunch(b->par[b->persist ? 1 : 0][par].graph, b->st));
     for (ocfd_handle* h : b->m) {
       std::swap(h->f, h->fn);
       std::swap(h->prim[4], h->talt);
@@ -1720,6 +1945,13 @@ int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
     BCK(cudaStreamSynchronize(b->st));
     for (ocfd_handle* h : b->m) {
       int r = ocfd_gpu_sync(h);
+      if (r == OCFD_E_TIMEOUT && b->persist) {
+        // a dependency wait of the persistent kernel gave up: later steps use
+        // one launch per kernel
+        b->pmode = 0;
+        b->persist = false;
+        b->f0.clear();
+      }
       if (r) return bfail(b, r, h->err);
     }
   }
@@ -1731,8 +1963,10 @@ void ocfd_batch_destroy(ocfd_batch* b) {
   cudaSetDevice(b->device);
   if (b->st) cudaStreamSynchronize(b->st);
   for (int P = 0; P < 2; P++) {
-    if (b->par[P].graph) cudaGraphExecDestroy(b->par[P].graph);
-    if (b->par[P].dev) cudaFree(b->par[P].dev);
+    for (int M = 0; M < 2; M++) {
+      if (b->par[M][P].graph) cudaGraphExecDestroy(b->par[M][P].graph);
+      if (b->par[M][P].dev) cudaFree(b->par[M][P].dev);
+    }
   }
   for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
   if (b->done) cudaEventDestroy(b->done);

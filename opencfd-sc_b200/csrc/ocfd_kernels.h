@@ -114,6 +114,38 @@ __device__ __forceinline__ const A& batch_args(const BatchTab<A>& b, int q, A* s
   return *sa;
 }
 
+// ---- persistent batched stage (ocfd_batch_stage.cuh): one launch per RK stage
+// item kinds
+enum { BW_FACE_X = 0, BW_FACE_Y = 1, BW_FACE_Z = 2, BW_VISC = 3, BW_TAIL = 4, BW_NEGT = 5 };
+
+// Tables of one stage launch (device memory; S = R in the batched paths).
+template <typename R>
+struct StageTab {
+  const FaceArgs<R>* face[3];   // per member, one stage's face-sweep arguments
+  const ViscArgs<R, R>* visc;   // per member
+  const UpdArgs<R>* upd;        // per member (tail)
+  const UpdArgs<double>* negt;  // per member (repair)
+  const int4* seg;              // segments by first item: {first item, member * 8 + kind, x extent, y extent}
+  const int2* need;             // per member: {phase-A items, tail items}
+  int* ctr;                     // [0] next item, [1 + q] phase-A items done, [1 + n + q] tail items done;
+                                // zero at launch
+  int nseg, nitems, count;
+};
+
+// Whether a persistent stage kernel exists for this combination.
+// scheme: OCFD_SCHEME_* (flux-vector WENO7 and characteristic OMP6, viscous).
+inline bool batch_stage_supported(bool chr, int scheme, bool visc) {
+  return visc && ((!chr && scheme == 2) || (chr && scheme == 3));
+}
+
+// One stage launch of nblocks persistent blocks; nblocks == 0 sets the kernel's
+// shared-memory limit and returns its resident blocks per SM in *per_sm (call
+// outside graph capture).  cudaErrorNotSupported: no persistent kernel for the
+// combination.
+template <typename R>
+cudaError_t launch_batch_stage(bool chr, int scheme, int variant, const StageTab<R>& t, int nblocks, cudaStream_t st,
+                               int* per_sm);
+
 template <typename R, typename S>
 cudaError_t launch_face(int dir, bool chr, int scheme, const FaceArgs<S>& a, cudaStream_t st);
 template <typename R, typename S>
@@ -152,7 +184,7 @@ template <typename R, typename S>
 cudaError_t launch_visc_grad_batch(const BatchTab<ViscArgs<R, S>>& b, int nblocks, cudaStream_t st);
 template <typename R>
 cudaError_t launch_fused_batch(const BatchTab<UpdArgs<R>>& b, int nblocks, bool chr, bool visc, bool fuse_bc,
-                               cudaStream_t st);
+                               bool i32, cudaStream_t st);
 cudaError_t launch_negt_fix_batch(const BatchTab<UpdArgs<double>>& b, cudaStream_t st);
 inline dim3 update_dims(const Grid& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
 

@@ -126,6 +126,12 @@ def _declare(L: C.CDLL) -> C.CDLL:
     L.ocfd_batch_set_tiles.restype = C.c_int
     L.ocfd_batch_info.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.ocfd_batch_info.restype = C.c_int
+    L.ocfd_batch_set_persistent.argtypes = [H, C.c_int]
+    L.ocfd_batch_set_persistent.restype = C.c_int
+    L.ocfd_batch_mode.argtypes = [H]
+    L.ocfd_batch_mode.restype = C.c_int
+    L.ocfd_batch_mode_times.argtypes = [H, C.POINTER(C.c_float)]
+    L.ocfd_batch_mode_times.restype = C.c_int
     L.ocfd_batch_last_error.argtypes = [H]
     L.ocfd_batch_last_error.restype = C.c_char_p
     L.ocfd_show_flow_msg_noalloc.argtypes = [P, C.c_void_p, C.c_void_p * 5, C.c_void_p, C.c_void_p, dp]
@@ -157,5 +163,6 @@ EXPORTED = [
     "ocfd_batch_set_tiles", "ocfd_batch_info", "ocfd_batch_last_error", "ocfd_gpu_metric_zero_mask",
     "ocfd_gpu_set_bc_layer", "ocfd_gpu_ana_q", "ocfd_gpu_ana_time_average", "ocfd_gpu_download_average",
     "ocfd_gpu_upload_average", "ocfd_gpu_ana_corner", "ocfd_gpu_download_block", "ocfd_gpu_step_kernels",
-    "ocfd_gpu_init_mesh_jacobian",
+    "ocfd_gpu_init_mesh_jacobian", "ocfd_batch_set_persistent", "ocfd_batch_mode",
+    "ocfd_batch_mode_times",
 ]

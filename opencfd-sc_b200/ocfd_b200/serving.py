@@ -128,7 +128,10 @@ class Server:
         # rather than all at the end (lower time to result)
         self.max_points = max_points
         self.hbm_budget = hbm_budget if hbm_budget is not None else _free_device_memory(device) * 85 // 100
-        self.tiles: dict[tuple, list] = {}  # face tile variants per set of grid sizes (autotuned once)
+        # per set of grid sizes: the face tile variants and the launch mode (one
+        # launch per kernel or one persistent launch per stage), chosen by timing
+        # on the first batch of those sizes and reused
+        self.tiles: dict[tuple, tuple] = {}
         _lib.lib()  # fail loudly here if the library is not built
 
     def run(self, requests: list[Request], realtime: bool = True, payloads: dict | None = None) -> dict:
@@ -165,34 +168,53 @@ class Server:
         clock = lambda: time.perf_counter() - t0
         arrival = (lambda r: r.arrival) if realtime else (lambda r: 0.0)
         waiting = list(reqs)
-        active: list[dict] = []
+        active: list[dict] = []   # admitted, with steps left to enqueue
         results: dict[int, Result] = {}
         used = 0
         batch = None
         members_key = None
-        rounds = batched_rounds = max_active = 0
-        while waiting or active:
-            # 1. launch the next round of the active instances (asynchronous)
-            k = 0
-            tuned_now = None
-            if active:
-                key = tuple(a["req"].rid for a in active)
+        in_flight = None          # (batch, members finishing with it, stale batch or None) of the enqueued round
+        rounds = batched_rounds = persistent_rounds = max_active = 0
+        while waiting or active or in_flight:
+            # 1. enqueue the next round of the active instances (asynchronous; on
+            # the GPU it follows the round in flight, which is not waited for)
+            run = [a for a in active if a["left"] > 0]
+            flight = None
+            if run:
+                key = tuple(a["req"].rid for a in run)
+                stale = None
+                tuned_now = None
                 if key != members_key:
-                    if batch is not None:
-                        batch.close()
-                    batch = Batch([a["s"] for a in active])
+                    stale = batch  # closed once its round has been retired
+                    batch = Batch([a["s"] for a in run])
                     members_key = key
-                    sizes = tuple(sorted({a["req"].n for a in active}))
+                    sizes = tuple(sorted({a["req"].n for a in run}))
                     if sizes in self.tiles:
-                        batch.set_tiles(self.tiles[sizes])
+                        variants, mode = self.tiles[sizes]
+                        batch.set_tiles(variants)
+                        if mode is not None:
+                            batch.set_persistent(mode == 2)
+                        else:
+                            tuned_now = sizes  # the launch mode is still to be timed
                     else:
                         tuned_now = sizes
-                k = min(self.round_steps, min(a["left"] for a in active))
+                k = min(self.round_steps, min(a["left"] for a in run))
                 batch.step(k, sync=False)
-                max_active = max(max_active, len(active))
+                rounds += 1
+                fused, variants = batch.info()
+                batched_rounds += 1 if fused else 0
+                persistent_rounds += 1 if batch.mode() == 2 else 0
+                if tuned_now is not None and fused:
+                    # the launch mode is kept once it was timed (a round of at least four steps)
+                    self.tiles[tuned_now] = (variants, batch.mode() if batch.mode_times() is not None else None)
+                for a in run:
+                    a["left"] -= k
+                max_active = max(max_active, len(run))
+                flight = (batch, [a for a in run if a["left"] == 0], stale)
             # 2. while it runs: admit arrived requests (FIFO) into free slots and memory
             new: list[dict] = []
             now = clock()
+            busy = len(run) > 0 or in_flight is not None
             while waiting and arrival(waiting[0]) <= now and len(active) + len(new) < self.max_slots:
                 r = waiting[0]
                 with ready:
@@ -200,8 +222,8 @@ class Server:
                         ready.wait(0.05)
                     p, xyz, prims = prepared[r.rid]
                 need = footprint(set_parameters(p))
-                pts = sum(a["req"].n ** 3 for a in active + new)
-                if (active or new) and (used + need > self.hbm_budget or pts + r.n ** 3 > self.max_points):
+                pts = sum(a["req"].n ** 3 for a in active + new if a["left"] > 0)
+                if (busy or new) and (used + need > self.hbm_budget or pts + r.n ** 3 > self.max_points):
                     break
                 with ready:
                     prepared.pop(r.rid)
@@ -210,35 +232,31 @@ class Server:
                 s = _start(p, xyz, prims, self.device)
                 used += need
                 new.append({"req": r, "s": s, "left": r.steps, "admitted": clock(), "bytes": need})
-            # 3. end of the round: results of the finished instances, slots freed
-            still = []
-            if k:
-                batch.step(0, sync=True)
-                rounds += 1
-                fused, variants = batch.info()
-                batched_rounds += 1 if fused else 0
-                if tuned_now is not None and fused:
-                    self.tiles[tuned_now] = variants
-                done_t = clock()
-                for a in active:
-                    a["left"] -= k
-                    if a["left"] > 0:
-                        still.append(a)
-                        continue
+            # 3. retire the previous round: results of the instances that finished
+            # with it (their streams follow it; the round enqueued above keeps
+            # the GPU busy meanwhile), their slots and memory freed
+            if in_flight is not None:
+                ob, fin, ostale = in_flight
+                for a in fin:
                     r, s = a["req"], a["s"]
+                    s.sync()  # negative-temperature status of the finished request
+                    E0 = s.show_flow_msg().tolist()
                     st = s.download_state() if r.rid in self.keep else None
-                    results[r.rid] = Result(rid=r.rid, arrival=arrival(r), admitted=a["admitted"], finished=done_t,
-                                            steps=r.steps, points=r.n ** 3, E0=s.show_flow_msg().tolist(), state=st)
-                if len(still) != len(active):
-                    batch.close()
-                    batch = None
-                    members_key = None
-                    for a in active:
-                        if a["left"] <= 0:
-                            a["s"].close()
-                            used -= a["bytes"]
-            active = still + new
-            if not active and waiting:
+                    results[r.rid] = Result(rid=r.rid, arrival=arrival(r), admitted=a["admitted"], finished=clock(),
+                                            steps=r.steps, points=r.n ** 3, E0=E0, state=st)
+                if ostale is not None:
+                    ostale.close()
+                if ob is not batch and (flight is None or flight[2] is not ob):
+                    ob.close()
+                if fin:
+                    done = {id(a) for a in fin}
+                    for a in fin:
+                        a["s"].close()
+                        used -= a["bytes"]
+                    active = [a for a in active if id(a) not in done]
+            in_flight = flight
+            active = active + new
+            if not run and in_flight is None and not new and waiting:
                 time.sleep(max(0.0, min(arrival(waiting[0]) - clock(), 0.5)))
         if batch is not None:
             batch.close()
@@ -249,7 +267,8 @@ class Server:
         ttr = np.array([r.time_to_result for r in results.values()])
         return {"results": results, "span_s": span, "gpts_per_s": work_pts / span / 1e9,
                 "p50_s": float(np.percentile(ttr, 50)), "p99_s": float(np.percentile(ttr, 99)),
-                "rounds": rounds, "batched_rounds": batched_rounds, "max_active": max_active}
+                "rounds": rounds, "batched_rounds": batched_rounds, "persistent_rounds": persistent_rounds,
+                "max_active": max_active}
 
 
 def run_sequential(requests: list[Request], mixed: bool = False, device: int = 0, keep=(),

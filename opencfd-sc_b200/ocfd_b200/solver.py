@@ -299,8 +299,9 @@ class Solver:
 
 class Batch:
     """Several solver instances advanced together (ocfd_batch_*): one launch per
-    kernel and RK stage for all of them when their configuration allows it,
-    bit-identical to stepping each alone."""
+    kernel and RK stage for all of them when their configuration allows it (one
+    persistent launch per stage for the flux-vector WENO7 and characteristic
+    OMP6 forms), bit-identical to stepping each alone."""
 
     def __init__(self, members: list[Solver]):
         if not members:
@@ -329,6 +330,30 @@ class Batch:
     def set_tiles(self, variants):
         v = (C.c_int * 3)(*variants)
         self._check(self.L.ocfd_batch_set_tiles(self.b, v), "batch_set_tiles")
+
+    def set_persistent(self, on):
+        """Launch mode where the persistent stage kernel exists: None (the
+        default) keeps the faster of the two, timed on the first steps; True:
+        one persistent launch per RK stage; False: one launch per kernel and
+        stage."""
+        v = -1 if on is None else (1 if on else 0)
+        self._check(self.L.ocfd_batch_set_persistent(self.b, v), "batch_set_persistent")
+
+    def mode_times(self):
+        """Device ms of the two steps timed per launch mode (per kernel,
+        persistent) by the launch-mode choice, or None before it ran."""
+        ms = (C.c_float * 2)()
+        if self.L.ocfd_batch_mode_times(self.b, ms) != 0:
+            return None
+        return float(ms[0]), float(ms[1])
+
+    def mode(self) -> int:
+        """0: members on their own graphs, 1: one batched launch per kernel and
+        stage, 2: one persistent launch per stage."""
+        r = self.L.ocfd_batch_mode(self.b)
+        if r < 0:
+            self._check(r, "batch_mode")
+        return r
 
     def info(self):
         fused = C.c_int()

@@ -1,8 +1,11 @@
 """Batched ensemble (GPU, through the C ABI): ragged periodic instances with
-different Re, Ma and dt advanced by one launch per kernel and RK stage give
-the same bits as each instance stepped alone, for both tile variants, with
-members used on their own between batch steps, and on the concurrent
-fallback path for configurations the batched launch does not cover."""
+different Re, Ma and dt advanced by one persistent launch per RK stage (the
+flux-vector WENO7 and characteristic OMP6 forms) or one launch per kernel and
+RK stage give the same bits as each instance stepped alone, for both tile
+variants, with members used on their own between batch steps, with the
+negative-temperature repair inside the persistent launch, and on the
+concurrent fallback path for configurations the batched launch does not
+cover."""
 import numpy as np
 import pytest
 
@@ -66,6 +69,14 @@ def test_batch_equals_alone(scheme, character, mixed, split):
     b.step(5)
     fused, variants = b.info()
     assert fused
+    if scheme == SCHEME_HYBRID:
+        assert b.mode() == 1
+    else:
+        # five steps: the launch mode was chosen by timing two steps in each
+        assert b.mode() in (1, 2)
+        t = b.mode_times()
+        assert t is not None and min(t) > 0
+        assert b.mode() == (2 if t[1] < t[0] else 1)
     for s, r in zip(members, ref):
         _same(s.download_state(), r)
         assert s.time()[0] == 5
@@ -133,3 +144,63 @@ def test_batch_fallback_for_walls():
     b.close()
     s1.close()
     s2.close()
+
+
+def _ragged_weno7_mixed(count):
+    sizes = [16, 24, 32, 40, 48]
+    return [_params((sizes[q % 5], sizes[(q + 2) % 5], sizes[(q + 4) % 5]), q % 4, SCHEME_WENO7, 0, True)
+            for q in range(count)]
+
+
+def test_persistent_stage_many_members():
+    """Twelve ragged members in the served configuration (flux-vector WENO7,
+    mixed precision): the persistent launch per stage, the launch per kernel and
+    each member alone give the same bits."""
+    ps = _ragged_weno7_mixed(12)
+    ref = _alone(ps, 4)
+    for persistent in (True, False):
+        members = [_make(p) for p in ps]
+        b = Batch(members)
+        b.set_persistent(persistent)
+        assert b.mode() == (2 if persistent else 1)
+        b.step(4)
+        for s, r in zip(members, ref):
+            _same(s.download_state(), r)
+        b.close()
+        for s in members:
+            s.close()
+
+
+def _planted(p):
+    """A member whose state has negative internal energy at two points: every
+    stage finds T <= 0 there and repairs it (handle_NegativeT)."""
+    s = _make(p)
+    f = s.download_f()
+    for (k, j, i) in [(3, 4, 5), (7, 2, 9)]:
+        f[4, k, j, i] = 0.3 * (f[1, k, j, i] ** 2 + f[2, k, j, i] ** 2 + f[3, k, j, i] ** 2) / f[0, k, j, i]
+    s.upload_state(f=f)
+    s.comput_duvwT()
+    return s
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
+def test_persistent_stage_negative_temperature_repair(mixed):
+    ps = [_params(sh, q, SCHEME_OMP6, 1, mixed) for q, sh in enumerate(SHAPES[:3])]
+    ref = []
+    for q, p in enumerate(ps):
+        s = _planted(p) if q == 1 else _make(p)
+        s.step(2)
+        ref.append(s.download_state())
+        if q == 1:
+            assert s.comput_duvwT() > 0  # the planted points stay negative: the stages repaired them
+        s.close()
+    members = [_planted(p) if q == 1 else _make(p) for q, p in enumerate(ps)]
+    b = Batch(members)
+    b.set_persistent(True)
+    assert b.mode() == 2
+    b.step(2)
+    for s, r in zip(members, ref):
+        _same(s.download_state(), r)
+    b.close()
+    for s in members:
+        s.close()

@@ -1,0 +1,58 @@
+"""Taylor-Green vortex 256^3, characteristic flux path, OMP6 and the hybrid
+with shock sensor 1, 500 time steps (GPU production build, through the C ABI)
+against the oracle's run of the same decks (tests/golden/tgv256_history.npz,
+made by tests/golden/make_tgv256_history.py): the show_flow_msg averages and
+the ana_box statistics every 5 steps, and the conserved state after the last
+step on every 16th point.
+
+Stated tolerance (FP64 path): 1e-10 relative on the kinetic energy and the
+state after the stated step count; the ana_box statistics, whose dissipation
+terms are derivatives of a developing field, within 1e-8."""
+import os
+
+import numpy as np
+import pytest
+
+from ocfd_b200 import cases
+from ocfd_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "tgv256_history.npz")
+
+
+def _rel(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+def _colerr(a, b):
+    """Per column: largest difference over the history relative to the
+    column's largest magnitude (columns that are identically zero compare
+    absolutely)."""
+    scale = np.maximum(np.max(np.abs(b), axis=0), 1e-300)
+    return np.max(np.abs(a - b), axis=0) / np.where(np.max(np.abs(b), axis=0) > 0, scale, 1.0)
+
+
+@pytest.mark.skipif(not os.path.exists(FIXTURE), reason="the 256^3 oracle history has not been generated")
+@pytest.mark.parametrize("scheme", ["OMP6", "HYBRID"])
+def test_tgv256_history_against_oracle(scheme):
+    g = np.load(FIXTURE)
+    key = scheme.lower()
+    steps, msg, box, f_sub = g[f"{key}_steps"], g[f"{key}_flow_msg"], g[f"{key}_ana_box"], g[f"{key}_f_sub"]
+    every, sub = int(g["every"]), int(g["sub"])
+    p = cases.tgv_char_params(256, scheme, dt=float(g["dt"]), steps=int(steps[-1]))
+    s = Solver(p)
+    s.init_mesh()
+    s.init3d(cases.tgv_prims(s.p))
+    m, b = [s.show_flow_msg()], [s.ana_box()]
+    for _ in steps[1:]:
+        s.step(every)
+        m.append(s.show_flow_msg())
+        b.append(s.ana_box())
+    f = s.download_f()[:, ::sub, ::sub, ::sub]
+    s.close()
+    m, b = np.array(m), np.array(b)
+    assert np.max(_rel(m[:, 1], msg[:, 1])) < 1e-10, "kinetic energy history"
+    assert np.max(_colerr(m, msg)) < 1e-10, "show_flow_msg history"
+    assert np.max(_colerr(b, box)) < 1e-8, "ana_box history"
+    assert np.linalg.norm(f - f_sub) / np.linalg.norm(f_sub) < 1e-10, "state after the last step"

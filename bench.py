@@ -659,6 +659,7 @@ def run_serve(args):
         "error_vs_fp64": {"sample": len(sample), **agg(mixed_err)},
         "fp64_perturbed_2^-24_vs_fp64": agg(floor_err),
         "scheme": "WENO7 flux-vector, SW, CD6; dt at CFL 0.5 from the initial field",
+        "grouping": f"instances of {srv.solo_min}^3 points and more on their own step graphs, smaller ones batched",
     }
     print(json.dumps(line), flush=True)
     return 0

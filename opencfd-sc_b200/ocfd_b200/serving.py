@@ -114,7 +114,8 @@ class Server:
     """Continuous-batching request loop on one device."""
 
     def __init__(self, device: int = 0, mixed: bool = True, hbm_budget: int | None = None, max_slots: int = 96,
-                 round_steps: int = 25, keep=(), prefetch: int = 16, max_points: int = 6_000_000):
+                 round_steps: int = 25, keep=(), prefetch: int = 16, max_points: int = 6_000_000,
+                 solo_min: int = 96):
         from . import _lib
 
         self.device = device
@@ -127,6 +128,12 @@ class Server:
         # run at full rate), few enough that requests finish in arrival order
         # rather than all at the end (lower time to result)
         self.max_points = max_points
+        # instances of at least solo_min^3 points advance on their own captured
+        # step graphs (single-instance kernels, concurrently on their own
+        # streams): measured faster than their part of a batched launch; the
+        # smaller ones share the batched launches, which run several of them at
+        # once where alone each would leave most of the GPU idle
+        self.solo_min = solo_min
         self.hbm_budget = hbm_budget if hbm_budget is not None else _free_device_memory(device) * 85 // 100
         # per set of grid sizes: the face tile variants and the launch mode (one
         # launch per kernel or one persistent launch per stage), chosen by timing
@@ -181,14 +188,19 @@ class Server:
             run = [a for a in active if a["left"] > 0]
             flight = None
             if run:
-                key = tuple(a["req"].rid for a in run)
+                k = min(self.round_steps, min(a["left"] for a in run))
+                solo = [a for a in run if a["req"].n >= self.solo_min]
+                grouped = [a for a in run if a["req"].n < self.solo_min]
+                for a in solo:
+                    a["s"].step(k, sync=False)
+                key = tuple(a["req"].rid for a in grouped)
                 stale = None
                 tuned_now = None
-                if key != members_key:
+                if grouped and key != members_key:
                     stale = batch  # closed once its round has been retired
-                    batch = Batch([a["s"] for a in run])
+                    batch = Batch([a["s"] for a in grouped])
                     members_key = key
-                    sizes = tuple(sorted({a["req"].n for a in run}))
+                    sizes = tuple(sorted({a["req"].n for a in grouped}))
                     if sizes in self.tiles:
                         variants, mode = self.tiles[sizes]
                         batch.set_tiles(variants)
@@ -198,19 +210,19 @@ class Server:
                             tuned_now = sizes  # the launch mode is still to be timed
                     else:
                         tuned_now = sizes
-                k = min(self.round_steps, min(a["left"] for a in run))
-                batch.step(k, sync=False)
                 rounds += 1
-                fused, variants = batch.info()
-                batched_rounds += 1 if fused else 0
-                persistent_rounds += 1 if batch.mode() == 2 else 0
-                if tuned_now is not None and fused:
-                    # the launch mode is kept once it was timed (a round of at least four steps)
-                    self.tiles[tuned_now] = (variants, batch.mode() if batch.mode_times() is not None else None)
+                if grouped:
+                    batch.step(k, sync=False)
+                    fused, variants = batch.info()
+                    batched_rounds += 1 if fused else 0
+                    persistent_rounds += 1 if batch.mode() == 2 else 0
+                    if tuned_now is not None and fused:
+                        # the launch mode is kept once it was timed (a round of at least four steps)
+                        self.tiles[tuned_now] = (variants, batch.mode() if batch.mode_times() is not None else None)
                 for a in run:
                     a["left"] -= k
                 max_active = max(max_active, len(run))
-                flight = (batch, [a for a in run if a["left"] == 0], stale)
+                flight = (batch if grouped else None, [a for a in run if a["left"] == 0], stale)
             # 2. while it runs: admit arrived requests (FIFO) into free slots and memory
             new: list[dict] = []
             now = clock()
@@ -246,7 +258,7 @@ class Server:
                                             steps=r.steps, points=r.n ** 3, E0=E0, state=st)
                 if ostale is not None:
                     ostale.close()
-                if ob is not batch and (flight is None or flight[2] is not ob):
+                if ob is not None and ob is not batch and (flight is None or flight[2] is not ob):
                     ob.close()
                 if fin:
                     done = {id(a) for a in fin}

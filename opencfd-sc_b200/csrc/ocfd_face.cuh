@@ -592,10 +592,18 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       using B = TmaBox<DIR, NP, TF, S>;
       const int e = DIR == 0 ? p * B::BX + l + toff : l * B::BX + p + toff;
       d = R(tile[e]);
-      u = R(tile[B::SLOT_ELEMS + e]);
-      v = R(tile[2 * B::SLOT_ELEMS + e]);
-      w = R(tile[3 * B::SLOT_ELEMS + e]);
-      T = R(tile[4 * B::SLOT_ELEMS + e]);
+      if constexpr (sizeof(S) == 4) {  // slots 1-4: the interleaved u,v,w,T tile
+        const float4 t = reinterpret_cast<const float4*>(tile + B::SLOT_ELEMS)[e];
+        u = R(t.x);
+        v = R(t.y);
+        w = R(t.z);
+        T = R(t.w);
+      } else {
+        u = R(tile[B::SLOT_ELEMS + e]);
+        v = R(tile[2 * B::SLOT_ELEMS + e]);
+        w = R(tile[3 * B::SLOT_ELEMS + e]);
+        T = R(tile[4 * B::SLOT_ELEMS + e]);
+      }
       const int m0 = 13 + 3 * DIR;
       if constexpr (AXS) {
         A1 = DIR == 0 ? R(tile[5 * B::SLOT_ELEMS + e]) : R(0);
@@ -1258,8 +1266,16 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
       if (need[q]) bytes += B::BYTES;
     }
     mbar_arrive_expect_tx(&bar, bytes);
-    for (int q = 0; q < 8; q++)
-      if (need[q]) tma_load_3d(tile + q * B::SLOT_ELEMS, &tm.m[q], c0, c1, c2, &bar);
+    if constexpr (sizeof(S) == 4) {
+      // FP32: d, then u,v,w,T interleaved (one 4-D copy filling slots 1-4)
+      tma_load_3d(tile, &tm.m[0], c0, c1, c2, &bar);
+      tma_load_4d(tile + B::SLOT_ELEMS, &tm.m[1], 0, c0, c1, c2, &bar);
+      for (int q = 5; q < 8; q++)
+        if (need[q]) tma_load_3d(tile + q * B::SLOT_ELEMS, &tm.m[q], c0, c1, c2, &bar);
+    } else {
+      for (int q = 0; q < 8; q++)
+        if (need[q]) tma_load_3d(tile + q * B::SLOT_ELEMS, &tm.m[q], c0, c1, c2, &bar);
+    }
   }
   // bounded wait (about a second); a block that gives up records the error and
   // waits once more, again bounded, for its copies before leaving
@@ -1332,7 +1348,10 @@ dim3 face_batch_dims(int dir, int variant, const FaceArgs<S>& a) {
 
 // ---- TMA path: tensor maps of the sweep's eight input arrays
 bool face_tma_enabled();
+bool face_tma32_enabled();
 bool encode_tile_map(CUtensorMap* map, const void* base, bool f64, const Grid& g, int bx, int by, int bz);
+// 4-D map of the interleaved FP32 u,v,w,T copy (4 floats a haloed point), box (4, bx, by, bz)
+bool encode_tile_map4(CUtensorMap* map, const void* base, const Grid& g, int bx, int by, int bz);
 
 template <typename S>
 inline bool tma_strides_ok(const Grid& g) {
@@ -1347,17 +1366,25 @@ static cudaError_t launch_face_tma_t(const FaceArgs<S>& a, cudaStream_t st) {
   auto kern = k_face_tma<DIR, CHAR, SCHEME, R, S, AXS, ALLIN>;
   if (a.g.n == 0) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   FaceTmaMaps tm;
+  memset(&tm, 0, sizeof(tm));
   const S* arr[8] = {a.d, a.u, a.v, a.w, a.T, a.A1, a.A2, a.A3};
-  for (int q = 0; q < 8; q++)
-    if (!encode_tile_map(&tm.m[q], arr[q], sizeof(S) == 8, a.g, B::BX, B::BY, B::BZ)) return cudaErrorInvalidValue;
+  for (int q = 0; q < 8; q++) {
+    bool ok = true;
+    if (sizeof(S) == 4 && q == 1)
+      ok = encode_tile_map4(&tm.m[1], a.q4, a.g, B::BX, B::BY, B::BZ);
+    else if (sizeof(S) == 8 || q == 0 || q >= 5)
+      ok = encode_tile_map(&tm.m[q], arr[q], sizeof(S) == 8, a.g, B::BX, B::BY, B::BZ);
+    if (!ok) return cudaErrorInvalidValue;
+  }
   kern<<<face_grid<DIR, NP, TF>(a), NP * TF, smem, st>>>(a, tm);
   return cudaGetLastError();
 }
 
-// One (direction, form, scheme) combination: the TMA-staged sweep for FP64
-// (periodic directions measured 1-3% faster at 256^3; the FP32 sweeps, four
-// blocks per SM, are as fast or faster with plain loads), the axis-aligned
-// variant when the metric row allows it (production build).  An empty grid
+// One (direction, form, scheme) combination: the TMA-staged sweep (FP64:
+// periodic directions measured 1-3% faster at 256^3; FP32 with the four
+// interleaved u,v,w,T floats of a point as the innermost dimension of a 4-D
+// copy), the axis-aligned variant when the metric row allows it (production
+// build).  An empty grid
 // asks for the shared-memory attribute of every variant instead.
 template <int D, bool C, int SC, typename R, typename S>
 static cudaError_t launch_face_dc(const FaceArgs<S>& a, cudaStream_t st) {
@@ -1366,25 +1393,19 @@ static cudaError_t launch_face_dc(const FaceArgs<S>& a, cudaStream_t st) {
     cudaError_t e = launch_face_t<D, C, SC, false, R, S>(a, st);
     if (e == cudaSuccess) e = launch_face_t<D, C, SC, true, R, S>(a, st);
     if (kAx && e == cudaSuccess) e = launch_face_t<D, C, SC, true, R, S, kAx>(a, st);
-    if constexpr (sizeof(S) == 8) {
-      if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S>(a, st);
-      if (kAx && e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, kAx>(a, st);
-      if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
-    }
+    if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S>(a, st);
+    if (kAx && e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, kAx>(a, st);
+    if (e == cudaSuccess) e = launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
     return e;
   }
   const bool allin = a.ph.periodic[D] != 0;
-  const bool tma = sizeof(S) == 8 && !a.no_tma && face_tma_enabled() && tma_strides_ok<S>(a.g);
+  const bool tma = !a.no_tma && (sizeof(S) == 8 ? face_tma_enabled() : face_tma32_enabled()) && tma_strides_ok<S>(a.g);
   if (!allin) {
-    if constexpr (sizeof(S) == 8) {
-      if (tma) return launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
-    }
+    if (tma) return launch_face_tma_t<D, C, SC, R, S, false, false>(a, st);
     return launch_face_t<D, C, SC, false, R, S>(a, st);
   }
   const bool ax = kAx && axis_aligned<D>(a.ph.metzero);
-  if constexpr (sizeof(S) == 8) {
-    if (tma) return ax ? launch_face_tma_t<D, C, SC, R, S, kAx>(a, st) : launch_face_tma_t<D, C, SC, R, S>(a, st);
-  }
+  if (tma) return ax ? launch_face_tma_t<D, C, SC, R, S, kAx>(a, st) : launch_face_tma_t<D, C, SC, R, S>(a, st);
   return ax ? launch_face_t<D, C, SC, true, R, S, kAx>(a, st) : launch_face_t<D, C, SC, true, R, S>(a, st);
 }
 

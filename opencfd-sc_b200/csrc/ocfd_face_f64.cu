@@ -35,6 +35,36 @@ bool face_tma_enabled() {
   return on == 1;
 }
 
+// TMA staging of the FP32 face sweeps: off unless OCFD_FACE_TMA32=1 (and the
+// driver offers a tensor-map encoder).  The FP32 sweeps compile to differently
+// contracted arithmetic in the TMA kernels than in the batched kernels (plain
+// loads), and a batched member must give the same bits as the same instance
+// stepped alone; the staged and the plain sweeps agree to FP32 rounding.
+bool face_tma32_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("OCFD_FACE_TMA32");
+    on = (e && e[0] == '1' && tile_encoder() != nullptr) ? 1 : 0;
+  }
+  return on == 1;
+}
+
+// Tiled 4-D map of the interleaved FP32 u,v,w,T copy (4 floats a haloed
+// point): dimensions (4, nxh, nyh, nzh), box (4, bx, by, bz) -- the innermost
+// box extent is the 16 bytes of one point, the point coordinates follow the
+// scalar maps.
+bool encode_tile_map4(CUtensorMap* map, const void* base, const Grid& g, int bx, int by, int bz) {
+  TileEncodeFn fn = tile_encoder();
+  if (!fn) return false;
+  const cuuint64_t dims[4] = {4, (cuuint64_t)g.nxh, (cuuint64_t)g.nyh, (cuuint64_t)g.nzh};
+  const cuuint64_t strides[3] = {16, (cuuint64_t)g.nxh * 16, (cuuint64_t)g.nxh * g.nyh * 16};
+  const cuuint32_t box[4] = {4, (cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Tiled 3-D map of a haloed (nxh, nyh, nzh) array, box (bx, by, bz); tiles
 // reaching past the array read zeros.
 bool encode_tile_map(CUtensorMap* map, const void* base, bool f64, const Grid& g, int bx, int by, int bz) {

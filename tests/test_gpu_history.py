@@ -7,7 +7,8 @@ step on every 16th point.
 
 Stated tolerance (FP64 path): 1e-10 relative on the kinetic energy and the
 state after the stated step count; the ana_box statistics, whose dissipation
-terms are derivatives of a developing field, within 1e-8."""
+terms are derivatives of a developing field, within 1e-8 of each statistic's
+largest value over the history."""
 import os
 
 import numpy as np
@@ -54,5 +55,11 @@ def test_tgv256_history_against_oracle(scheme):
     m, b = np.array(m), np.array(b)
     assert np.max(_rel(m[:, 1], msg[:, 1])) < 1e-10, "kinetic energy history"
     assert np.max(_colerr(m, msg)) < 1e-10, "show_flow_msg history"
-    assert np.max(_colerr(b, box)) < 1e-8, "ana_box history"
+    # ana_box columns (OCFD_ANA.f90:178-311 order): the velocity skewness <u^3>/u_rms^3
+    # (column 8) vanishes by the Taylor-Green symmetry -- both runs hold rounding
+    # residue of about 1e-11 there, compared in absolute terms
+    err = _colerr(b, box)
+    err[8] = 0.0
+    assert np.max(err) < 1e-8, "ana_box history"
+    assert np.max(np.abs(b[:, 8] - box[:, 8])) < 1e-12, "velocity skewness residue"
     assert np.linalg.norm(f - f_sub) / np.linalg.norm(f_sub) < 1e-10, "state after the last step"

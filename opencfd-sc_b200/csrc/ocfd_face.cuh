@@ -676,9 +676,10 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
         sm[SI(11, l, p)] = v;
         sm[SI(12, l, p)] = w;
         sm[SI(13, l, p)] = c;
-        sm[SI(14, l, p)] = A1;
-        sm[SI(15, l, p)] = A2;
-        sm[SI(16, l, p)] = A3;
+        // axis-aligned sweeps read only the direction's metric component
+        if (!AXS || DIR == 0) sm[SI(14, l, p)] = A1;
+        if (!AXS || DIR == 1) sm[SI(15, l, p)] = A2;
+        if (!AXS || DIR == 2) sm[SI(16, l, p)] = A3;
       }
     }
   }
@@ -914,20 +915,30 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
                 for (int v = 0; v < 4; v++) G[v] = xfma(oa[7 - q], f4[v], G[v]);
                 G[4] = xfma(oa[7 - q], W(4, q), G[4]);
               }
-            } else {
-#pragma unroll
-              for (int v = 0; v < 5; v++) {
-                R acc = xmul(oa[0], W(v, 7));
-#pragma unroll
-                for (int q = 6; q >= 0; q--) acc = xfma(oa[7 - q], W(v, q), acc);
-                G[v] = acc;
-              }
             }
-            proj5v(G[0], G[1], G[2], G[3], G[4], dP);
             R pa[5], pb[5], pc[5];
-            proj5(0, 2, pa);
-            proj5(0, 3, pb);
-            proj5(0, 4, pc);
+            if constexpr (PS > 1) {
+              proj5v(G[0], G[1], G[2], G[3], G[4], dP);
+              proj5(0, 2, pa);
+              proj5(0, 3, pb);
+              proj5(0, 4, pc);
+            } else {
+              // point by point: the three points of the monotonicity test are
+              // projected from the values the stencil sum loaded (one
+              // shared-memory read of each point)
+#pragma unroll
+              for (int q = 7; q >= 0; q--) {
+                R f[5];
+#pragma unroll
+                for (int v = 0; v < 5; v++) f[v] = W(v, q);
+#pragma unroll
+                for (int v = 0; v < 5; v++) G[v] = q == 7 ? xmul(oa[0], f[v]) : xfma(oa[7 - q], f[v], G[v]);
+                if (q == 4) proj5v(f[0], f[1], f[2], f[3], f[4], pc);
+                if (q == 3) proj5v(f[0], f[1], f[2], f[3], f[4], pb);
+                if (q == 2) proj5v(f[0], f[1], f[2], f[3], f[4], pa);
+              }
+              proj5v(G[0], G[1], G[2], G[3], G[4], dP);
+            }
 #pragma unroll
             for (int r = 0; r < 5; r++) {
               const R mp = xadd(pb[r], minmod2(xadd(pc[r], -pb[r]), xmul(kap, xadd(pb[r], -pa[r]))));
@@ -950,20 +961,27 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
                 for (int v = 0; v < 4; v++) G[v] = xfma(oa[q], f4[v], G[v]);
                 G[4] = xfma(oa[q], W(9, q), G[4]);
               }
+            }
+            R pa[5], pb[5], pc[5];
+            if constexpr (PS > 1) {
+              proj5v(G[0], G[1], G[2], G[3], G[4], dM);
+              proj5(5, 3, pa);
+              proj5(5, 4, pb);
+              proj5(5, 5, pc);
             } else {
 #pragma unroll
-              for (int v = 0; v < 5; v++) {
-                R acc = xmul(oa[0], W(5 + v, 0));
+              for (int q = 0; q <= 7; q++) {
+                R f[5];
 #pragma unroll
-                for (int q = 1; q <= 7; q++) acc = xfma(oa[q], W(5 + v, q), acc);
-                G[v] = acc;
+                for (int v = 0; v < 5; v++) f[v] = W(5 + v, q);
+#pragma unroll
+                for (int v = 0; v < 5; v++) G[v] = q == 0 ? xmul(oa[0], f[v]) : xfma(oa[q], f[v], G[v]);
+                if (q == 3) proj5v(f[0], f[1], f[2], f[3], f[4], pa);
+                if (q == 4) proj5v(f[0], f[1], f[2], f[3], f[4], pb);
+                if (q == 5) proj5v(f[0], f[1], f[2], f[3], f[4], pc);
               }
+              proj5v(G[0], G[1], G[2], G[3], G[4], dM);
             }
-            proj5v(G[0], G[1], G[2], G[3], G[4], dM);
-            R pa[5], pb[5], pc[5];
-            proj5(5, 3, pa);
-            proj5(5, 4, pb);
-            proj5(5, 5, pc);
 #pragma unroll
             for (int r = 0; r < 5; r++) {
               const R mp = xadd(pb[r], minmod2(xadd(pa[r], -pb[r]), xmul(kap, xadd(pb[r], -pc[r]))));

@@ -22,6 +22,12 @@ over FP64 and its errors against the FP64 run (kinetic energy and enstrophy
 histories, relative L2 / Linf of rho, u and p) after the workload's stated
 number of steps, both runs from the same initial field.
 
+The same line carries a "served" object: a compact seeded stream of 64
+mixed-size requests served with continuous batching (aggregate GPts/s, p50/p99
+time to result) against the same requests solved one after another in FP64
+and in mixed precision (`--serve` runs the full 256-request stream with errors
+against FP64).
+
 Multi-GPU: the path does not shard in this build (one grid per GPU); N GPUs run
 N independent replicas ("replicas only", weak scaling), the time is the max
 over ranks and the value is the total grid-point updates of all ranks.
@@ -525,6 +531,9 @@ def run_ours(args):
     else:
         s.close()
     del prims, xyz
+    served = None
+    if args.workload in WORKLOADS and not args.no_serve and world == 1:
+        served = served_leg()
 
     line = None
     if rank == 0:
@@ -565,6 +574,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, **kern,
                          "note": "the face kernels are FP64-pipe (FP64) or issue (FP32) bound, not HBM bound"},
             "mixed": mixed,
+            "served": served,
             "cpu_baseline": cpu,
             "kinetic_energy": ke,
         }
@@ -573,6 +583,33 @@ def run_ours(args):
         tdist.barrier()
         tdist.destroy_process_group()
     return 0
+
+
+def served_leg(count: int = 64, rate: float = 16.0, steps=(100, 300)) -> dict:
+    """A compact served stream for the default bench line: `count` seeded Poisson
+    requests (TGV / isotropic turbulence, 32^3-128^3, mixed precision, served with
+    continuous batching), against the same requests solved one after another in
+    FP64 and in mixed precision.  Host clock (time to result is wall time)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from ocfd_b200 import serving
+
+    reqs = serving.make_stream(count, rate=rate, seed=20261204, steps=steps)
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        prepared = list(ex.map(lambda r: serving.request_setup(r, True), reqs))
+    payloads = {r.rid: x for r, x in zip(reqs, prepared)}
+    served = serving.Server(mixed=True).run(reqs, realtime=True, payloads=payloads)
+    seq = serving.run_sequential(reqs, mixed=False, payloads=payloads)
+    seq_m = serving.run_sequential(reqs, mixed=True, payloads=payloads)
+    pick = lambda d: {k: d[k] for k in ("gpts_per_s", "p50_s", "p99_s", "span_s")}
+    return {"requests": count, "rate_per_s": rate, "steps": list(steps),
+            "work_gpt_steps": int(sum(r.n ** 3 * r.steps for r in reqs)),
+            "served_mixed": pick(served) | {"rounds": served["rounds"]},
+            "sequential_fp64": pick(seq), "sequential_mixed": pick(seq_m),
+            "served_over_sequential_fp64": served["gpts_per_s"] / seq["gpts_per_s"],
+            "served_over_sequential_mixed": served["gpts_per_s"] / seq_m["gpts_per_s"],
+            "note": "results bit-identical alone and in the mix; the full 256-request stream with errors "
+                    "against FP64 is the --serve mode"}
 
 
 def run_serve(args):
@@ -724,6 +761,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of an FP64 line")
+    ap.add_argument("--no-serve", action="store_true", help="skip the compact served-stream leg")
     ap.add_argument("--err-steps", type=int, default=None,
                     help="horizon of the mixed-vs-FP64 errors (default: the workload's stated step count)")
     ap.add_argument("--serve", action="store_true", help="served request stream instead of the step benchmark")

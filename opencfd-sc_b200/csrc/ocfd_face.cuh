@@ -902,6 +902,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           {
             // per component: oa[0] F(7) + oa[1] F(6) + ... + oa[7] F(0), in this order
             R G[5];
+            R pa[5], pb[5], pc[5];
             if constexpr (PS > 1) {  // point by point, four components a load
               R f4[4];
               W4(0, 7, f4);
@@ -911,17 +912,16 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #pragma unroll
               for (int q = 6; q >= 0; q--) {
                 W4(0, q, f4);
+                const R f5 = W(4, q);
 #pragma unroll
                 for (int v = 0; v < 4; v++) G[v] = xfma(oa[7 - q], f4[v], G[v]);
-                G[4] = xfma(oa[7 - q], W(4, q), G[4]);
+                G[4] = xfma(oa[7 - q], f5, G[4]);
+                // the points of the monotonicity test, projected from these loads
+                if (q == 4) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pc);
+                if (q == 3) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pb);
+                if (q == 2) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pa);
               }
-            }
-            R pa[5], pb[5], pc[5];
-            if constexpr (PS > 1) {
               proj5v(G[0], G[1], G[2], G[3], G[4], dP);
-              proj5(0, 2, pa);
-              proj5(0, 3, pb);
-              proj5(0, 4, pc);
             } else {
               // point by point: the three points of the monotonicity test are
               // projected from the values the stencil sum loaded (one
@@ -948,6 +948,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           {
             // per component: oa[0] F(0) + oa[1] F(1) + ... + oa[7] F(7), in this order
             R G[5];
+            R pa[5], pb[5], pc[5];
             if constexpr (PS > 1) {
               R f4[4];
               W4(5, 0, f4);
@@ -957,17 +958,15 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #pragma unroll
               for (int q = 1; q <= 7; q++) {
                 W4(5, q, f4);
+                const R f5 = W(9, q);
 #pragma unroll
                 for (int v = 0; v < 4; v++) G[v] = xfma(oa[q], f4[v], G[v]);
-                G[4] = xfma(oa[q], W(9, q), G[4]);
+                G[4] = xfma(oa[q], f5, G[4]);
+                if (q == 3) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pa);
+                if (q == 4) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pb);
+                if (q == 5) proj5v(f4[0], f4[1], f4[2], f4[3], f5, pc);
               }
-            }
-            R pa[5], pb[5], pc[5];
-            if constexpr (PS > 1) {
               proj5v(G[0], G[1], G[2], G[3], G[4], dM);
-              proj5(5, 3, pa);
-              proj5(5, 4, pb);
-              proj5(5, 5, pc);
             } else {
 #pragma unroll
               for (int q = 0; q <= 7; q++) {

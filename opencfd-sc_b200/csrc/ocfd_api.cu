@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -1531,6 +1532,12 @@ static int batch_capture(ocfd_batch* b, int parity, bool persist) {
       for (int d = 0; d < 3; d++) c += add(q, BW_FACE_X + d, face_batch_dims<S>(d, b->vstage, face_args<S>(M[q], d)));
       if (h0->p.if_viscous) c += add(q, BW_VISC, update_dims(M[q]->g));
       need[q].x = c;
+      // test of the bounded dependency waits: OCFD_TEST_STALL_BATCH_WAIT=1
+      // lists one phase-A item more than the member has, so that its tail
+      // items' waits cannot complete (the kernel must give up, record error 5
+      // and finish; the host reports OCFD_E_TIMEOUT)
+      const char* stall = std::getenv("OCFD_TEST_STALL_BATCH_WAIT");
+      if (stall && stall[0] == '1') need[q].x += 1;
     };
     auto tail = [&](int q) { need[q].y = add(q, BW_TAIL, update_dims(M[q]->g)); };
     // A0 A1 T0 A2 T1 ... A(n-1) T(n-2) T(n-1), then the repairs: everything an
@@ -1943,6 +1950,10 @@ int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
   for (ocfd_handle* h : b->m) BCK(cudaStreamWaitEvent(h->st, b->done, 0));
   if (sync) {
     BCK(cudaStreamSynchronize(b->st));
+    // every member's status is read (and a timeout's error word cleared) before
+    // the first failure is returned
+    int first = OCFD_OK;
+    std::string msg;
     for (ocfd_handle* h : b->m) {
       int r = ocfd_gpu_sync(h);
       if (r == OCFD_E_TIMEOUT && b->persist) {
@@ -1952,8 +1963,12 @@ int ocfd_batch_step(ocfd_batch* b, int nsteps, int sync) {
         b->persist = false;
         b->f0.clear();
       }
-      if (r) return bfail(b, r, h->err);
+      if (r && first == OCFD_OK) {
+        first = r;
+        msg = h->err;
+      }
     }
+    if (first) return bfail(b, first, msg);
   }
   return OCFD_OK;
 }

@@ -204,3 +204,34 @@ def test_persistent_stage_negative_temperature_repair(mixed):
     b.close()
     for s in members:
         s.close()
+
+
+def test_persistent_stage_wait_timeout_is_reported(monkeypatch):
+    """The dependency waits of the persistent launch are bounded: with a work
+    list whose phase-A counts cannot be reached (a test switch read when the
+    tables are built), the kernel gives up after about a second, finishes, and
+    the step reports OCFD_E_TIMEOUT; the batch then continues with one launch
+    per kernel, with no error left behind (restarted from the initial field,
+    the members give the same bits as alone)."""
+    from ocfd_b200._lib import OCFD_E_TIMEOUT, OcfdError
+
+    ps = _ragged_weno7_mixed(2)
+    members = [_make(p) for p in ps]
+    b = Batch(members)
+    b.set_persistent(True)
+    monkeypatch.setenv("OCFD_TEST_STALL_BATCH_WAIT", "1")
+    with pytest.raises(OcfdError) as err:
+        b.step(1)
+    assert err.value.code == OCFD_E_TIMEOUT
+    monkeypatch.delenv("OCFD_TEST_STALL_BATCH_WAIT")
+    assert b.mode() == 1
+    # the timed-out step left invalid states: start again from the initial field
+    ref = _alone(ps, 2)
+    for s in members:
+        s.init3d(cases.tgv_prims(s.p))
+    b.step(2)
+    for s, r in zip(members, ref):
+        _same(s.download_state(), r)
+    b.close()
+    for s in members:
+        s.close()

@@ -743,6 +743,12 @@ static FaceArgs<S> face_args(ocfd_handle* h, int d) {
   a.split = h->p.flux_splitting;
   a.err = &h->dstat->error;
   a.no_tma = h->tma_off ? 1 : 0;
+  // test of the bounded TMA waits: OCFD_TEST_STALL_TMA=1 makes the staged
+  // sweeps expect 16 bytes more than their copies deliver, so that no wait can
+  // complete (the blocks give up, record error 4 and leave; the host reports
+  // OCFD_E_TIMEOUT and stages with plain loads from then on)
+  const char* stall = std::getenv("OCFD_TEST_STALL_TMA");
+  a.test_tx = (stall && stall[0] == '1') ? 16 : 0;
   return a;
 }
 

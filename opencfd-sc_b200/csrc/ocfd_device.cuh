@@ -272,6 +272,7 @@ struct FaceArgs {
   int split;         // 1 SW, 2 LLF
   int* err;          // DevStatus::error of the instance (bounded waits record 4 there)
   int no_tma;        // host side: stage the tile with plain loads (a TMA wait of this instance gave up)
+  int test_tx;       // 0; test of the bounded TMA waits: bytes the staging expects beyond its copies
   Phys ph;
 };
 

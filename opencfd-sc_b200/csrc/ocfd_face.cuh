@@ -1282,7 +1282,7 @@ __global__ void OCFD_FACE_BOUNDS k_face_tma(FaceArgs<S> a, const __grid_constant
       need[q] = q < 5 || !((a.ph.metzero >> (m0 + q - 5)) & 1u);
       if (need[q]) bytes += B::BYTES;
     }
-    mbar_arrive_expect_tx(&bar, bytes);
+    mbar_arrive_expect_tx(&bar, bytes + (uint32_t)a.test_tx);
     if constexpr (sizeof(S) == 4) {
       // FP32: d, then u,v,w,T interleaved (one 4-D copy filling slots 1-4)
       tma_load_3d(tile, &tm.m[0], c0, c1, c2, &bar);

@@ -471,7 +471,9 @@ __device__ __forceinline__ void negt_fix_body(const UpdArgs<double>& a) {
   st->negt_count = 0;
   st->negt_total += cnt;
   if (cnt > 10) {
-    st->error = 3;
+    // a gave-up wait of this step (4, 5) is the cause to report: it stays
+    const int prev = __ldcg(&st->error);
+    if (prev != 4 && prev != 5) st->error = 3;
     return;
   }
   int idx[16];

@@ -1573,7 +1573,11 @@ static int batch_capture(ocfd_batch* b, int parity, bool persist) {
     BCK(cudaMalloc(&P.dev, im.buf.size()));
     P.bytes = im.buf.size();
   }
-  BCK(cudaMemcpy(P.dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice));
+  // on the batch stream, so that the launches reading the tables follow the
+  // copy (a synchronous copy runs on the legacy stream, which the batch's
+  // non-blocking stream is not ordered after: it may return before its DMA
+  // has landed); from pageable memory the call returns once the image is staged
+  BCK(cudaMemcpyAsync(P.dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice, b->st));
   unsigned char* base = (unsigned char*)P.dev;
   auto tab = [&](size_t args_off, size_t ent_off) {
     struct {
@@ -1699,7 +1703,11 @@ static int batch_autotune(ocfd_batch* b) {
         rc = bfail(b, OCFD_E_NOMEM, "autotune table");
         break;
       }
-      cudaMemcpy(dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice);
+      // on the timed stream: the launches below follow the copy
+      if (cudaMemcpyAsync(dev, im.buf.data(), im.buf.size(), cudaMemcpyHostToDevice, b->st) != cudaSuccess) {
+        rc = bfail(b, OCFD_E_CUDA, "autotune table upload");
+        break;
+      }
       BatchTab<FaceArgs<S>> bt = {(const FaceArgs<S>*)((unsigned char*)dev + oa),
                                   (const int4*)((unsigned char*)dev + oe), n};
       float tot = 0.f;
@@ -1707,8 +1715,9 @@ static int batch_autotune(ocfd_batch* b) {
         cudaEventRecord(e0, b->st);
         cudaError_t e = launch_face_batch<R, S>(d, h0->chr, h0->p.scheme_invis, v, bt, nblk, b->st);
         cudaEventRecord(e1, b->st);
-        if (e != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
-          rc = bfail(b, OCFD_E_CUDA, "autotune launch");
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+          rc = bfail(b, OCFD_E_CUDA, std::string("autotune launch: ") + cudaGetErrorString(e));
           break;
         }
         float ms = 0.f;

@@ -354,8 +354,10 @@ int ocfd_gpu_download_block(ocfd_handle* h, int ib, int ie, int jb, int je, int 
  * blocks: nz above OCFD_NOALLOC_MAX_PLANES is rejected with OCFD_E_PARAM.
  * Nothing in that array has to start at zero.  The first call on a device,
  * made with that device current, looks up the array's address (once per
- * device) and keeps it for the life of the process; make that first call
- * before any stream capture begins.  A cudaDeviceReset of that device makes
+ * device) and keeps it for the life of the process.  No call may be made
+ * while its stream is capturing (the call copies to host memory and waits):
+ * a capturing stream is refused with OCFD_E_PARAM before anything is
+ * enqueued.  A cudaDeviceReset of that device makes
  * the kept address stale: do not use this entry point on a device after
  * resetting it.  There is one array per device, so overlapping calls on the
  * same device (from several streams or host threads) race: serialise them. */

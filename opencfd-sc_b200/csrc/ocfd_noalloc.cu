@@ -129,6 +129,11 @@ extern "C" int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f,
                  p->nz, OCFD_NOALLOC_MAX_PLANES);
     return OCFD_E_PARAM;
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  // the copy to host memory and the wait below cannot be captured
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return OCFD_E_CUDA;
+  if (cs != cudaStreamCaptureStatusNone) return OCFD_E_PARAM;
   double* scratch = nullptr;
   int r = scratch_for_current_device(&scratch);
   if (r) return r;
@@ -141,7 +146,6 @@ extern "C" int ocfd_show_flow_msg_noalloc(const ocfd_params* p, const double* f,
   G.nzh = p->nz + 2 * ocfd::LAP;
   G.n = (long long)G.nx * G.ny * G.nz;
   G.nh = (long long)G.nxh * G.nyh * G.nzh;
-  cudaStream_t st = (cudaStream_t)stream;
   double* part = scratch;
   double* total = scratch + 3 * OCFD_NOALLOC_MAX_PLANES;
   // row bands per plane: about four blocks per SM of a B200 over the whole

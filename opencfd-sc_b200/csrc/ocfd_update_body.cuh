@@ -13,9 +13,12 @@
 // Minimum resident blocks per SM requested for the viscous-gradient and
 // stage-tail kernels (both memory-latency bound: more resident warps keep
 // more loads in flight, at the price of registers).  Measured best on B200 at
-// 256^3: FP64 tail 4, FP32 tail 5 (with the interleaved viscous fluxes; 5 and
-// 6 before), FP64 viscous 4, FP32 viscous 6 (against 2-3 blocks with the
-// compiler's own register choice).
+// 256^3: FP64 tail 5 (with the 256-bit viscous-flux loads; 3 / 4 / 6 blocks:
+// 3.93 / 3.63 / 4.37 against 3.60 ms per step), FP32 tail 5 (with the
+// interleaved viscous fluxes; 5 and 6 before), FP64 viscous 4 (3 / 5 / 6
+// blocks: 3.48 / 4.04 / 5.49 against 2.76 ms per step: fewer warps expose the
+// stencil-load latency, more spill), FP32 viscous 6 (against 2-3 blocks with
+// the compiler's own register choice).
 #ifndef OCFD_VISC64_MINB
 #define OCFD_VISC64_MINB 4
 #endif
@@ -23,12 +26,17 @@
 #define OCFD_VISC32_MINB 6
 #endif
 #ifndef OCFD_TAIL64_MINB
-#define OCFD_TAIL64_MINB 4
+#define OCFD_TAIL64_MINB 5
 #endif
 #ifndef OCFD_TAIL32_MINB
 #define OCFD_TAIL32_MINB 5
 #endif
 #define OCFD_VISC_MINB (sizeof(R) == 8 ? OCFD_VISC64_MINB : OCFD_VISC32_MINB)
+// FP64 viscous fluxes (four components of a point, 32 bytes) moved by single
+// 256-bit global loads and stores
+#ifndef OCFD_V256
+#define OCFD_V256 1
+#endif
 #define OCFD_TAIL_MINB (sizeof(R) == 8 ? OCFD_TAIL64_MINB : OCFD_TAIL32_MINB)
 
 namespace ocfd {
@@ -72,19 +80,31 @@ template <typename R>
 __device__ __forceinline__ V4<R> operator/(const V4<R>& a, R c) {
   return V4<R>{{a.v[0] / c, a.v[1] / c, a.v[2] / c, a.v[3] / c}};
 }
-// the four components of one point of an interleaved viscous-flux array
+// the four components of one point of an interleaved viscous-flux array (32
+// bytes, 32-byte aligned: the arrays start on 256-byte boundaries).
+// OCFD_V256: one 256-bit access (sm_100) in place of two 16-byte ones.
 __device__ __forceinline__ V4<double> ldg4(const double* p) {
+#if OCFD_V256
+  double a, b, c, d;
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+  return V4<double>{{a, b, c, d}};
+#else
   const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
   return V4<double>{{a.x, a.y, b.x, b.y}};
+#endif
 }
 __device__ __forceinline__ V4<float> ldg4(const float* p) {
   const float4 a = __ldg(reinterpret_cast<const float4*>(p));
   return V4<float>{{a.x, a.y, a.z, a.w}};
 }
 __device__ __forceinline__ void st4(double* p, double a, double b, double c, double d) {
+#if OCFD_V256
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+#else
   // two 16-byte stores (four scalar stores measured 10% slower in the viscous kernel)
   reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
   reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+#endif
 }
 __device__ __forceinline__ void st4(float* p, float a, float b, float c, float d) {
   *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);

@@ -702,6 +702,55 @@ def run_serve(args):
     return 0
 
 
+def run_batched(args):
+    """Steady-state throughput of batched mixed-precision steps (the serving
+    path's WENO7 flux-vector form) per member set, in both launch modes (one
+    launch per kernel and RK stage; one persistent launch per stage), beside
+    the members stepped one after another alone.  Host clock over --steps steps
+    after --warmup (synchronised on both sides), GPts/s."""
+    import time
+
+    from ocfd_b200 import serving
+    from ocfd_b200.solver import Batch
+
+    def members(sizes):
+        out = []
+        for q, n in enumerate(sizes):
+            r = serving.Request(rid=q, kind="tgv" if q % 2 == 0 else "hit", n=n, re=1600.0, ma=0.3,
+                                steps=10 ** 6, arrival=0.0, seed=1000 + q)
+            p, xyz, prims = serving.request_setup(r, True)
+            out.append(serving._start(p, xyz, prims, 0))
+        return out
+
+    sets = {"64 x 32^3": [32] * 64, "19 x 48^3": [48] * 19, "8 x 64^3": [64] * 8, "2 x 96^3": [96] * 2,
+            "1 x 128^3": [128], "12 ragged 32^3-128^3": [32, 48, 64, 96, 128, 32, 48, 64, 32, 48, 64, 128]}
+    res = {}
+    for name, sizes in sets.items():
+        ms = members(sizes)
+        pts = sum(n ** 3 for n in sizes)
+        row = {}
+        for mode in (False, True):
+            b = Batch(ms)
+            b.set_persistent(mode)
+            b.step(args.warmup)
+            t0 = time.perf_counter()
+            b.step(args.steps)
+            row["persistent" if mode else "per_kernel"] = pts * args.steps / (time.perf_counter() - t0) / 1e9
+            b.close()
+        for s in ms:
+            s.step(args.warmup)
+        t0 = time.perf_counter()
+        for s in ms:
+            s.step(args.steps)  # each alone on its own step graph, one after another
+        row["single"] = pts * args.steps / (time.perf_counter() - t0) / 1e9
+        for s in ms:
+            s.close()
+        res[name] = {k: round(v, 4) for k, v in row.items()}
+    print(json.dumps({"metric": "batched mixed WENO7 steady state", "unit": "GPts/s", "steps": args.steps,
+                      "warmup": args.warmup, "sets": res}), flush=True)
+    return 0
+
+
 def run_history(args):
     """Kinetic-energy, dissipation-rate (-dK/dt) and enstrophy histories of the
     256^3 characteristic TGV runs (OMP6 and hybrid): the GPU production build
@@ -768,6 +817,8 @@ def main():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--round-steps", type=int, default=25)
+    ap.add_argument("--batched", action="store_true",
+                    help="steady-state batched throughput per member set (both launch modes) instead")
     ap.add_argument("--history", action="store_true", help="kinetic-energy / dissipation histories vs the oracle")
     ap.add_argument("--hist-steps", type=int, default=500)
     ap.add_argument("--hist-oracle-steps", type=int, default=20)
@@ -781,6 +832,8 @@ def main():
         return run_serve(args)
     if args.history:
         return run_history(args)
+    if args.batched:
+        return run_batched(args)
     return run_ours(args)
 
 

@@ -403,6 +403,33 @@ struct CharBasis {
   }
 };
 
+// CharBasis::proj (c = L f) of two points at once, in the two lanes of packed
+// FP32 operations; each lane performs proj's own explicitly rounded operations
+// (a negation is a product with -1, which is exact), so both lanes give proj's
+// bits.
+template <int DIR, bool AXS>
+__device__ __forceinline__ void char_proj2(const CharBasis<DIR, AXS, float>& b, const F2* f, float KK, float KK1,
+                                           float X1, float V2_, float un_, float ul_, float um_, F2* cc) {
+  const F2 A = add2(fma2(f2(-b.w), f[3], fma2(f2(-b.v), f[2], fma2(f2(-b.u), f[1], mul2(f2(V2_), f[0])))), f[4]);
+  cc[0] = fma2(f2(-KK), A, f[0]);
+  const F2 KA = mul2(f2(KK1), A);
+  if constexpr (AXS) {
+    constexpr int LI = CharBasis<DIR, AXS, float>::LI, MI = CharBasis<DIR, AXS, float>::MI;
+    const F2 B = fma2(f2(-b.n1), f[1 + DIR], mul2(f2(un_), f[0]));
+    cc[1] = fma2(f2(-ul_), f[0], mul2(f2(b.sl()), f[1 + LI]));
+    cc[2] = fma2(f2(-um_), f[0], DIR == 2 ? mul2(f2(-1.0f), f[1 + MI]) : f[1 + MI]);
+    cc[3] = fma2(f2(X1), B, KA);
+    cc[4] = fma2(f2(-X1), B, KA);
+  } else {
+    const float m1_ = b.m1(), m2_ = b.m2(), m3_ = b.m3();
+    const F2 B = fma2(f2(-b.n3), f[3], fma2(f2(-b.n2), f[2], fma2(f2(-b.n1), f[1], mul2(f2(un_), f[0]))));
+    cc[1] = fma2(f2(-ul_), f[0], fma2(f2(b.l3), f[3], fma2(f2(b.l2), f[2], mul2(f2(b.l1), f[1]))));
+    cc[2] = fma2(f2(-um_), f[0], fma2(f2(m3_), f[3], fma2(f2(m2_), f[2], mul2(f2(m1_), f[1]))));
+    cc[3] = fma2(f2(X1), B, KA);
+    cc[4] = fma2(f2(-X1), B, KA);
+  }
+}
+
 // One queued limiter evaluation (OCFD_inviscous_character.f90:205-248 for the
 // face state and row r of the left eigenvector matrix, :256-270 for the
 // projection, OCFD_Schemes_1.f90:212-224 for the limiter): the face whose
@@ -750,13 +777,26 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       if (inner) {
 #pragma unroll 1
         for (int m = 0; m < 5; m++) {
-          R wv[8];
+          R h1, h2;
+          if constexpr (OCFD_F32X2 && sizeof(R) == 4 && SCHEME == SCH_WENO7) {
+            // production FP32: F+ and F- by one packed evaluation -- the F+
+            // window in lane x, the F- window mirrored (offset k holds F-(1-k))
+            // in lane y
+            F2 w2[7];
 #pragma unroll
-          for (int q = 0; q < 8; q++) wv[q] = W(m, q);
-          const R h1 = schemeP<SCHEME>(wv + 3, U, ihy);
+            for (int q = 0; q < 7; q++) w2[q] = f2(float(W(m, q)), float(W(5 + m, 7 - q)));
+            const float2 h = weno7_x2(w2);
+            h1 = h.x;
+            h2 = h.y;
+          } else {
+            R wv[8];
 #pragma unroll
-          for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
-          const R h2 = schemeM<SCHEME>(wv + 3, U, ihy);
+            for (int q = 0; q < 8; q++) wv[q] = W(m, q);
+            h1 = schemeP<SCHEME>(wv + 3, U, ihy);
+#pragma unroll
+            for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
+            h2 = schemeM<SCHEME>(wv + 3, U, ihy);
+          }
           if (OCFD_FV_SUMMED) {
             out[fo + (long long)m * a.fs] = h1 + h2;
           } else {
@@ -899,6 +939,71 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           // projected once -- and only the three points of the monotonicity test
           // are projected (results move by rounding only).  Components that fail
           // the test are queued for the block-wide limiter pass below.
+          if constexpr (OCFD_F32X2 && sizeof(R) == 4 && PS == 1) {
+            // production FP32, sweeps without point records (z): the F+ and F-
+            // blocks below in the two lanes of packed operations -- step s takes
+            // F+(7 - s) and F-(s), both with oa[s]; every lane operation is the
+            // blocks' own explicitly rounded operation, so the results are the
+            // same bits (z sweep at 256^3: 1.73 -> 1.65 ms per step).  The x and y
+            // sweeps (point records) keep the blocks one after the other: with
+            // both sides live they spill at 64 registers and measured slower
+            // (1.74 -> 1.92 ms), and at 85 registers slower still.
+            const F2 m1 = f2(-1.0f), kap2 = f2(float(kap));
+            // X4: the middle test point pb of both sides; MP: the test's bound
+            // mp = pb + minmod2(t1, kap t2) with t1 = pc - pb, t2 = pb - pa (F+)
+            // and t1 = pa - pb, t2 = pb - pc (F-), formed as the points arrive
+            F2 G2[5], X4[5], MP[5];
+#pragma unroll
+            for (int s = 0; s <= 7; s++) {
+              R fp[5], fm[5];
+              if constexpr (PS > 1) {
+                W4(0, 7 - s, fp);
+                fp[4] = W(4, 7 - s);
+                W4(5, s, fm);
+                fm[4] = W(9, s);
+              } else {
+#pragma unroll
+                for (int v = 0; v < 5; v++) {
+                  fp[v] = W(v, 7 - s);
+                  fm[v] = W(5 + v, s);
+                }
+              }
+              F2 f[5];
+#pragma unroll
+              for (int v = 0; v < 5; v++) f[v] = f2(float(fp[v]), float(fm[v]));
+              const F2 c = f2(float(oa[s]));
+#pragma unroll
+              for (int v = 0; v < 5; v++) G2[v] = s == 0 ? mul2(c, f[v]) : fma2(c, f[v], G2[v]);
+              // the points of the monotonicity test: step 3 holds F+ point 4 (pc)
+              // and F- point 3 (pa), step 4 pb of both, step 5 F+ point 2 (pa)
+              // and F- point 5 (pc)
+              if (s == 3) char_proj2(cb, f, KK, KK1, X1, V2, un, ul, um, MP);  // held in MP until step 4
+              if (s == 4) {
+                char_proj2(cb, f, KK, KK1, X1, V2, un, ul, um, X4);
+#pragma unroll
+                for (int r = 0; r < 5; r++) MP[r] = fma2(m1, X4[r], MP[r]);  // t1
+              }
+              if (s == 5) {
+                F2 X5[5];
+                char_proj2(cb, f, KK, KK1, X1, V2, un, ul, um, X5);
+#pragma unroll
+                for (int r = 0; r < 5; r++) {
+                  const F2 t2 = mul2(kap2, fma2(m1, X5[r], X4[r]));
+                  MP[r] = add2(X4[r], f2(minmod2(MP[r].v.x, t2.v.x), minmod2(MP[r].v.y, t2.v.y)));
+                }
+              }
+            }
+            F2 D[5];
+            char_proj2(cb, G2, KK, KK1, X1, V2, un, ul, um, D);
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+              const F2 tt = mul2(fma2(m1, X4[r], D[r]), fma2(m1, MP[r], D[r]));
+              dfl |= (tt.v.x >= float(ep) ? 1u : 0u) << r;
+              dfl |= (tt.v.y >= float(ep) ? 1u : 0u) << (5 + r);
+              dP[r] = D[r].v.x;
+              dM[r] = D[r].v.y;
+            }
+          } else {
           {
             // per component: oa[0] F(7) + oa[1] F(6) + ... + oa[7] F(0), in this order
             R G[5];
@@ -986,6 +1091,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
               const R mp = xadd(pb[r], minmod2(xadd(pa[r], -pb[r]), xmul(kap, xadd(pb[r], -pc[r]))));
               dfl |= (xmul(xadd(dM[r], -pb[r]), xadd(dM[r], -mp)) >= ep ? 1u : 0u) << (5 + r);
             }
+          }
           }
           if (dfl) {
             // queue entries djb, djb+1, ... in the order (r, F+ then F-)

@@ -217,6 +217,71 @@ __device__ __forceinline__ R weno7M(const R* v) {
   return weno_sum4(ep, C0, C1, C2, C3, S0, S1, S2, S3, q0, q1, q2, q3);
 }
 
+// ---- packed FP32 (production mixed path, sm_100): two reconstructions per
+// instruction.  FFMA2 / FADD2 / FMUL2 apply one IEEE single-precision operation,
+// rounded to nearest, to each of two lanes; the issue-bound FP32 face sweeps
+// issue half the arithmetic instructions.  Lanes round as the scalar operations
+// would, but the contraction into FMAs is fixed here rather than left to the
+// compiler, so results can differ from the scalar form in the last bits; the
+// batched and single-instance sweeps share this code and agree bit for bit.
+#ifndef OCFD_F32X2
+#define OCFD_F32X2 OCFD_FEWER_DIVS
+#endif
+struct F2 {
+  float2 v;
+};
+__device__ __forceinline__ F2 f2(float a) { return F2{make_float2(a, a)}; }
+__device__ __forceinline__ F2 f2(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ F2 add2(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+
+// WENO7 of two windows at once: w[0..6] are the stencil values at offsets -3..3
+// of weno7P.  Lane x: F+ (weno7P of the F+ window); lane y: F- -- weno7M(v) is
+// weno7P of the mirrored window v'(k) = v(1 - k), term for term, so the caller
+// puts F-(1 - k) in lane y of w[k + 3].  Same terms and order as weno7P; the
+// weights' divisions are per lane.
+__device__ __forceinline__ float2 weno7_x2(const F2* w) {
+  const F2 C0 = f2(float(1.0 / 35.0)), C1 = f2(float(12.0 / 35.0)), C2 = f2(float(18.0 / 35.0)), C3 = f2(float(4.0 / 35.0));
+  const F2 m1 = f2(-1.0f), b2 = f2(-2.0f), c3 = f2(3.0f);
+  const F2 *v = w + 3;
+  // S1k, S2k, S3k: weno7P's smoothness differences
+  F2 S10 = fma2(f2(float(11.0 / 6.0)), v[0], fma2(f2(float(-18.0 / 6.0)), v[-1], fma2(f2(float(9.0 / 6.0)), v[-2], mul2(f2(float(-2.0 / 6.0)), v[-3]))));
+  F2 S11 = fma2(f2(float(2.0 / 6.0)), v[1], fma2(f2(float(3.0 / 6.0)), v[0], fma2(m1, v[-1], mul2(f2(float(1.0 / 6.0)), v[-2]))));
+  F2 S12 = fma2(f2(float(-1.0 / 6.0)), v[2], add2(fma2(f2(float(-3.0 / 6.0)), v[0], mul2(f2(float(-2.0 / 6.0)), v[-1])), v[1]));
+  F2 S13 = fma2(f2(float(2.0 / 6.0)), v[3], fma2(f2(float(-9.0 / 6.0)), v[2], fma2(f2(float(18.0 / 6.0)), v[1], mul2(f2(float(-11.0 / 6.0)), v[0]))));
+  F2 S20 = fma2(f2(2.0f), v[0], fma2(f2(-5.0f), v[-1], fma2(f2(4.0f), v[-2], mul2(m1, v[-3]))));
+  F2 S21 = add2(fma2(b2, v[0], v[-1]), v[1]);
+  F2 S22 = add2(fma2(b2, v[1], v[0]), v[2]);
+  F2 S23 = fma2(m1, v[3], fma2(f2(4.0f), v[2], fma2(f2(-5.0f), v[1], mul2(f2(2.0f), v[0]))));
+  F2 S30 = add2(fma2(c3, fma2(m1, v[-1], v[-2]), mul2(m1, v[-3])), v[0]);
+  F2 S31 = add2(fma2(c3, fma2(m1, v[0], v[-1]), mul2(m1, v[-2])), v[1]);
+  F2 S32 = add2(fma2(c3, fma2(m1, v[1], v[0]), mul2(m1, v[-1])), v[2]);
+  F2 S33 = add2(fma2(c3, fma2(m1, v[2], v[1]), mul2(m1, v[0])), v[3]);
+  const F2 d12 = f2(float(13.0 / 12.0)), d13 = f2(float(1043.0 / 960.0)), d14 = f2(float(1.0 / 12.0));
+  auto beta = [&](F2 a, F2 b, F2 c) {
+    return fma2(mul2(d14, a), c, fma2(mul2(d13, c), c, fma2(mul2(d12, b), b, mul2(a, a))));
+  };
+  const F2 S0 = beta(S10, S20, S30), S1 = beta(S11, S21, S31), S2 = beta(S12, S22, S32), S3 = beta(S13, S23, S33);
+  // candidate values q0..q3
+  const F2 q0 = fma2(f2(float(25.0 / 12.0)), v[0], fma2(f2(float(-23.0 / 12.0)), v[-1], fma2(f2(float(13.0 / 12.0)), v[-2], mul2(f2(float(-3.0 / 12.0)), v[-3]))));
+  const F2 q1 = fma2(f2(float(3.0 / 12.0)), v[1], fma2(f2(float(13.0 / 12.0)), v[0], fma2(f2(float(-5.0 / 12.0)), v[-1], mul2(f2(float(1.0 / 12.0)), v[-2]))));
+  const F2 q2 = fma2(f2(float(-1.0 / 12.0)), v[2], fma2(f2(float(7.0 / 12.0)), v[1], fma2(f2(float(7.0 / 12.0)), v[0], mul2(f2(float(-1.0 / 12.0)), v[-1]))));
+  const F2 q3 = fma2(f2(float(1.0 / 12.0)), v[3], fma2(f2(float(-5.0 / 12.0)), v[2], fma2(f2(float(13.0 / 12.0)), v[1], mul2(f2(float(3.0 / 12.0)), v[0]))));
+  // weights a_k = C_k / (ep + S_k)^2 (divisions per lane), normalised sum
+  const F2 ep = f2(float(1.0e-8));
+  F2 D0 = add2(ep, S0), D1 = add2(ep, S1), D2 = add2(ep, S2), D3 = add2(ep, S3);
+  D0 = mul2(D0, D0);
+  D1 = mul2(D1, D1);
+  D2 = mul2(D2, D2);
+  D3 = mul2(D3, D3);
+  const F2 a0 = f2(C0.v.x / D0.v.x, C0.v.y / D0.v.y), a1 = f2(C1.v.x / D1.v.x, C1.v.y / D1.v.y);
+  const F2 a2 = f2(C2.v.x / D2.v.x, C2.v.y / D2.v.y), a3 = f2(C3.v.x / D3.v.x, C3.v.y / D3.v.y);
+  const F2 am = add2(add2(add2(a0, a1), a2), a3);
+  const F2 num = fma2(a3, q3, fma2(a2, q2, fma2(a1, q1, mul2(a0, q0))));
+  return make_float2(num.v.x / am.v.x, num.v.y / am.v.y);
+}
+
 // minmod2 / minmod4: OCFD_Schemes.f90:274-289
 // minmod2 = 0.5*(sign(1,x1) + sign(1,x2)) * min(|x1|, |x2|): the sign factor is
 // +-1 when the sign bits agree and 0 otherwise, so for finite arguments the

@@ -148,7 +148,13 @@ __global__ void __launch_bounds__(256, OCFD_FACE_MINB) k_batch_stage(StageTab<R>
           stage_face<2, CHAR, SCHEME, V, R>(*reinterpret_cast<const FaceArgs<R>*>(sa), bx, by, bz, sm);
           break;
         case BW_VISC:
-          if (VISC) visc_grad_body(*reinterpret_cast<const ViscArgs<R, R>*>(sa), bx, by, bz);
+          if (VISC) {
+            const ViscArgs<R, R>& A = *reinterpret_cast<const ViscArgs<R, R>*>(sa);
+            if (OCFD_VISC_AXS && visc_axis_aligned(A.ph.metzero))
+              visc_grad_body<R, R, OCFD_VISC_AXS != 0>(A, bx, by, bz);
+            else
+              visc_grad_body<R, R>(A, bx, by, bz);
+          }
           break;
         case BW_TAIL:
           fused_body<CHAR, VISC, true, R>(*reinterpret_cast<const UpdArgs<R>*>(sa), bx, by, bz);

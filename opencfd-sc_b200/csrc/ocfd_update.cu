@@ -49,31 +49,45 @@ static SlabOrder slab_order(const Grid& g) {
   return so;
 }
 
-template <typename R, typename S, bool SLAB>
+template <typename R, typename S, bool SLAB, bool AXS = false>
 __global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad(ViscArgs<R, S> a, SlabOrder so) {
   if (!SLAB) {
-    visc_grad_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+    visc_grad_body<R, S, AXS>(a, blockIdx.x, blockIdx.y, blockIdx.z);
     return;
   }
   int bx, by, bz;
   if (!slab_decode(so, a.g.nz, bx, by, bz)) return;
-  visc_grad_body(a, bx, by, bz);
+  visc_grad_body<R, S, AXS>(a, bx, by, bz);
 }
 template <typename R, typename S>
 __global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
   __shared__ __align__(16) ViscArgs<R, S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
-  visc_grad_body(batch_args(b, q, &sa), bx, by, bz);
+  const ViscArgs<R, S>& A = batch_args(b, q, &sa);
+  // the member's own variant, as its single-instance launch chooses it
+  if (OCFD_VISC_AXS && visc_axis_aligned(A.ph.metzero))
+    visc_grad_body<R, S, OCFD_VISC_AXS != 0>(A, bx, by, bz);
+  else
+    visc_grad_body<R, S>(A, bx, by, bz);
 }
 
 template <typename R, typename S>
 cudaError_t launch_visc_grad(const ViscArgs<R, S>& a, cudaStream_t st) {
   const SlabOrder so = slab_order(a.g);
-  if (so.sy == so.gy)
-    k_visc_grad<R, S, false><<<update_dims(a.g), 256, 0, st>>>(a, so);
-  else
-    k_visc_grad<R, S, true><<<slab_grid(so, a.g.nz), 256, 0, st>>>(a, so);
+  constexpr bool kAx = OCFD_VISC_AXS != 0;
+  const bool ax = kAx && visc_axis_aligned(a.ph.metzero);
+  if (so.sy == so.gy) {
+    if (ax)
+      k_visc_grad<R, S, false, kAx><<<update_dims(a.g), 256, 0, st>>>(a, so);
+    else
+      k_visc_grad<R, S, false><<<update_dims(a.g), 256, 0, st>>>(a, so);
+  } else {
+    if (ax)
+      k_visc_grad<R, S, true, kAx><<<slab_grid(so, a.g.nz), 256, 0, st>>>(a, so);
+    else
+      k_visc_grad<R, S, true><<<slab_grid(so, a.g.nz), 256, 0, st>>>(a, so);
+  }
   return cudaGetLastError();
 }
 template <typename R, typename S>

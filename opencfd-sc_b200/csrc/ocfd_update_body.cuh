@@ -140,7 +140,23 @@ __device__ __forceinline__ V d0(F at, int l, int nn, int periodic, int cd8, D0C<
 // ---------------------------------------------------------------------------
 // du_viscous part 1 (OCFD_viscous.f90:193-264): comput_Amu (:135-149), the 12
 // gradients, stress and heat flux, and the contravariant viscous fluxes Ev.
-template <typename R, typename S>
+// Whether every off-diagonal metric the viscous body reads is identically zero
+// (Aky Akz Aix Aiz Asx Asy of the gradients, Aky1 Akz1 Aix1 Aiz1 Asx1 Asy1 of the
+// fluxes): a grid whose axes are the coordinate axes (box, stretched box).
+#ifndef OCFD_VISC_AXS
+#define OCFD_VISC_AXS OCFD_FEWER_DIVS
+#endif
+__host__ __device__ __forceinline__ bool visc_axis_aligned(unsigned int metzero) {
+  const unsigned int off = (1u << 4) | (1u << 5) | (1u << 6) | (1u << 8) | (1u << 9) | (1u << 10) | (1u << 14) |
+                           (1u << 15) | (1u << 16) | (1u << 18) | (1u << 19) | (1u << 20);
+  return (metzero & off) == off;
+}
+
+// AXS (production build, visc_axis_aligned grids): the Cartesian gradients and
+// the contravariant fluxes take only the diagonal metrics -- the general form's
+// other terms add exact zeros, so the values are the same (up to the sign of a
+// zero) with a third of the metric registers and products.
+template <typename R, typename S, bool AXS = false>
 __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const int bx, const int by, const int bz) {
   const Grid& G = a.g;
   const int i = bx * 32 + (threadIdx.x & 31) + 1;
@@ -182,6 +198,40 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
         auto at = [&](int off) -> R { return R(__ldg(base + off * hs)); };
         gr[q][dir] = d0<R>(at, lcoord[dir], G.len(dir), a.ph.periodic[dir], cd8, d0c<R>(a.dc, dir));
       }
+  }
+  if constexpr (AXS) {
+    // metric indices (flow_data order): Akx 3, Aiy 7, Asz 11, Akx1 13, Aiy1 17, Asz1 21
+    const R Akx = R(__ldg(a.met[3] + c)), Aiy = R(__ldg(a.met[7] + c)), Asz = R(__ldg(a.met[11] + c));
+    const R ux = gr[0][0] * Akx, vx = gr[1][0] * Akx, wx = gr[2][0] * Akx, Tx = gr[3][0] * Akx;
+    const R uy = gr[0][1] * Aiy, vy = gr[1][1] * Aiy, wy = gr[2][1] * Aiy, Ty = gr[3][1] * Aiy;
+    const R uz = gr[0][2] * Asz, vz = gr[1][2] * Asz, wz = gr[2][2] * Asz, Tz = gr[3][2] * Asz;
+    const R div = ux + vy + wz;
+    const R Tsb = R(110.4 / a.ph.ref_amu_t0), TmpR = R(1.0 / a.ph.re);
+    if constexpr (sizeof(S) != 4) T = R(__ldg(a.T + c));
+    const R Amu = TmpR * (R(1) + Tsb) * sqrt(T * T * T) / (Tsb + T);
+    const R Amuk = R(a.ph.cp) * Amu / R(a.ph.pr);
+    const R t23 = R(2.0 / 3.0);
+    const R s11 = (R(2) * ux - t23 * div) * Amu;
+    const R s22 = (R(2) * vy - t23 * div) * Amu;
+    const R s33 = (R(2) * wz - t23 * div) * Amu;
+    const R s12 = (uy + vx) * Amu;
+    const R s13 = (uz + wx) * Amu;
+    const R s23 = (vz + wy) * Amu;
+    if constexpr (sizeof(S) != 4) {
+      uu = R(__ldg(a.u + c));
+      vv = R(__ldg(a.v + c));
+      ww = R(__ldg(a.w + c));
+    }
+    const R E1 = uu * s11 + vv * s12 + ww * s13 + Amuk * Tx;
+    const R E2 = uu * s12 + vv * s22 + ww * s23 + Amuk * Ty;
+    const R E3 = uu * s13 + vv * s23 + ww * s33 + Amuk * Tz;
+    const long long o = G.ii(i, j, k);
+    const long long n = G.n;
+    const R A1 = R(__ldg(a.met[13] + c)), A2 = R(__ldg(a.met[17] + c)), A3 = R(__ldg(a.met[21] + c));
+    st4(a.ev + o * 4, A1 * s11, A1 * s12, A1 * s13, A1 * E1);
+    st4(a.ev + (n + o) * 4, A2 * s12, A2 * s22, A2 * s23, A2 * E2);
+    st4(a.ev + (2 * n + o) * 4, A3 * s13, A3 * s23, A3 * s33, A3 * E3);
+    return;
   }
   R M[22];
 #pragma unroll

@@ -231,55 +231,55 @@ __device__ __forceinline__ void visc_grad_body(const ViscArgs<R, S>& a, const in
     st4(a.ev + o * 4, A1 * s11, A1 * s12, A1 * s13, A1 * E1);
     st4(a.ev + (n + o) * 4, A2 * s12, A2 * s22, A2 * s23, A2 * E2);
     st4(a.ev + (2 * n + o) * 4, A3 * s13, A3 * s23, A3 * s33, A3 * E3);
-    return;
-  }
-  R M[22];
+  } else {
+    R M[22];
 #pragma unroll
-  for (int m = 3; m < 22; m++) M[m] = met_at<R>(a.ph, m, a.met[m], c);
-  const R Akx = M[3], Aky = M[4], Akz = M[5], Aix = M[6], Aiy = M[7], Aiz = M[8], Asx = M[9], Asy = M[10],
-          Asz = M[11];
-  const R ux = gr[0][0] * Akx + gr[0][1] * Aix + gr[0][2] * Asx;
-  const R vx = gr[1][0] * Akx + gr[1][1] * Aix + gr[1][2] * Asx;
-  const R wx = gr[2][0] * Akx + gr[2][1] * Aix + gr[2][2] * Asx;
-  const R Tx = gr[3][0] * Akx + gr[3][1] * Aix + gr[3][2] * Asx;
-  const R uy = gr[0][0] * Aky + gr[0][1] * Aiy + gr[0][2] * Asy;
-  const R vy = gr[1][0] * Aky + gr[1][1] * Aiy + gr[1][2] * Asy;
-  const R wy = gr[2][0] * Aky + gr[2][1] * Aiy + gr[2][2] * Asy;
-  const R Ty = gr[3][0] * Aky + gr[3][1] * Aiy + gr[3][2] * Asy;
-  const R uz = gr[0][0] * Akz + gr[0][1] * Aiz + gr[0][2] * Asz;
-  const R vz = gr[1][0] * Akz + gr[1][1] * Aiz + gr[1][2] * Asz;
-  const R wz = gr[2][0] * Akz + gr[2][1] * Aiz + gr[2][2] * Asz;
-  const R Tz = gr[3][0] * Akz + gr[3][1] * Aiz + gr[3][2] * Asz;
-  const R div = ux + vy + wz;
-  // Sutherland viscosity, comput_Amu
-  const R Tsb = R(110.4 / a.ph.ref_amu_t0), TmpR = R(1.0 / a.ph.re);
-  if constexpr (sizeof(S) != 4) T = R(__ldg(a.T + c));
-  const R Amu = TmpR * (R(1) + Tsb) * sqrt(T * T * T) / (Tsb + T);
-  const R Amuk = R(a.ph.cp) * Amu / R(a.ph.pr);
-  const R t23 = R(2.0 / 3.0);
-  const R s11 = (R(2) * ux - t23 * div) * Amu;
-  const R s22 = (R(2) * vy - t23 * div) * Amu;
-  const R s33 = (R(2) * wz - t23 * div) * Amu;
-  const R s12 = (uy + vx) * Amu;
-  const R s13 = (uz + wx) * Amu;
-  const R s23 = (vz + wy) * Amu;
-  if constexpr (sizeof(S) != 4) {
-    uu = R(__ldg(a.u + c));
-    vv = R(__ldg(a.v + c));
-    ww = R(__ldg(a.w + c));
-  }
-  const R E1 = uu * s11 + vv * s12 + ww * s13 + Amuk * Tx;
-  const R E2 = uu * s12 + vv * s22 + ww * s23 + Amuk * Ty;
-  const R E3 = uu * s13 + vv * s23 + ww * s33 + Amuk * Tz;
-  const long long o = G.ii(i, j, k);
-  const long long n = G.n;
-  // Ev stored direction by direction, the four components of a point together:
-  // element (d, point o, component m) at (d*n + o)*4 + m
+    for (int m = 3; m < 22; m++) M[m] = met_at<R>(a.ph, m, a.met[m], c);
+    const R Akx = M[3], Aky = M[4], Akz = M[5], Aix = M[6], Aiy = M[7], Aiz = M[8], Asx = M[9], Asy = M[10],
+            Asz = M[11];
+    const R ux = gr[0][0] * Akx + gr[0][1] * Aix + gr[0][2] * Asx;
+    const R vx = gr[1][0] * Akx + gr[1][1] * Aix + gr[1][2] * Asx;
+    const R wx = gr[2][0] * Akx + gr[2][1] * Aix + gr[2][2] * Asx;
+    const R Tx = gr[3][0] * Akx + gr[3][1] * Aix + gr[3][2] * Asx;
+    const R uy = gr[0][0] * Aky + gr[0][1] * Aiy + gr[0][2] * Asy;
+    const R vy = gr[1][0] * Aky + gr[1][1] * Aiy + gr[1][2] * Asy;
+    const R wy = gr[2][0] * Aky + gr[2][1] * Aiy + gr[2][2] * Asy;
+    const R Ty = gr[3][0] * Aky + gr[3][1] * Aiy + gr[3][2] * Asy;
+    const R uz = gr[0][0] * Akz + gr[0][1] * Aiz + gr[0][2] * Asz;
+    const R vz = gr[1][0] * Akz + gr[1][1] * Aiz + gr[1][2] * Asz;
+    const R wz = gr[2][0] * Akz + gr[2][1] * Aiz + gr[2][2] * Asz;
+    const R Tz = gr[3][0] * Akz + gr[3][1] * Aiz + gr[3][2] * Asz;
+    const R div = ux + vy + wz;
+    // Sutherland viscosity, comput_Amu
+    const R Tsb = R(110.4 / a.ph.ref_amu_t0), TmpR = R(1.0 / a.ph.re);
+    if constexpr (sizeof(S) != 4) T = R(__ldg(a.T + c));
+    const R Amu = TmpR * (R(1) + Tsb) * sqrt(T * T * T) / (Tsb + T);
+    const R Amuk = R(a.ph.cp) * Amu / R(a.ph.pr);
+    const R t23 = R(2.0 / 3.0);
+    const R s11 = (R(2) * ux - t23 * div) * Amu;
+    const R s22 = (R(2) * vy - t23 * div) * Amu;
+    const R s33 = (R(2) * wz - t23 * div) * Amu;
+    const R s12 = (uy + vx) * Amu;
+    const R s13 = (uz + wx) * Amu;
+    const R s23 = (vz + wy) * Amu;
+    if constexpr (sizeof(S) != 4) {
+      uu = R(__ldg(a.u + c));
+      vv = R(__ldg(a.v + c));
+      ww = R(__ldg(a.w + c));
+    }
+    const R E1 = uu * s11 + vv * s12 + ww * s13 + Amuk * Tx;
+    const R E2 = uu * s12 + vv * s22 + ww * s23 + Amuk * Ty;
+    const R E3 = uu * s13 + vv * s23 + ww * s33 + Amuk * Tz;
+    const long long o = G.ii(i, j, k);
+    const long long n = G.n;
+    // Ev stored direction by direction, the four components of a point together:
+    // element (d, point o, component m) at (d*n + o)*4 + m
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const R A1 = M[13 + 3 * d], A2 = M[14 + 3 * d], A3 = M[15 + 3 * d];
-    st4(a.ev + ((long long)d * n + o) * 4, A1 * s11 + A2 * s12 + A3 * s13, A1 * s12 + A2 * s22 + A3 * s23,
-        A1 * s13 + A2 * s23 + A3 * s33, A1 * E1 + A2 * E2 + A3 * E3);
+    for (int d = 0; d < 3; d++) {
+      const R A1 = M[13 + 3 * d], A2 = M[14 + 3 * d], A3 = M[15 + 3 * d];
+      st4(a.ev + ((long long)d * n + o) * 4, A1 * s11 + A2 * s12 + A3 * s13, A1 * s12 + A2 * s22 + A3 * s23,
+          A1 * s13 + A2 * s23 + A3 * s33, A1 * E1 + A2 * E2 + A3 * E3);
+    }
   }
 }
 

@@ -115,7 +115,7 @@ class Server:
 
     def __init__(self, device: int = 0, mixed: bool = True, hbm_budget: int | None = None, max_slots: int = 96,
                  round_steps: int = 25, keep=(), prefetch: int = 16, max_points: int = 6_000_000,
-                 solo_min: int = 96):
+                 solo_min: int = 96, launch_mode: str = "timed"):
         from . import _lib
 
         self.device = device
@@ -134,6 +134,11 @@ class Server:
         # smaller ones share the batched launches, which run several of them at
         # once where alone each would leave most of the GPU idle
         self.solo_min = solo_min
+        # batched launch mode: "timed" (each new set of grid sizes times both modes
+        # on its first round and keeps the faster), "per_kernel" or "persistent"
+        if launch_mode not in ("timed", "per_kernel", "persistent"):
+            raise ValueError(f"launch_mode {launch_mode!r}")
+        self.launch_mode = launch_mode
         self.hbm_budget = hbm_budget if hbm_budget is not None else _free_device_memory(device) * 85 // 100
         # per set of grid sizes: the face tile variants and the launch mode (one
         # launch per kernel or one persistent launch per stage), chosen by timing
@@ -200,11 +205,13 @@ class Server:
                     stale = batch  # closed once its round has been retired
                     batch = Batch([a["s"] for a in grouped])
                     members_key = key
+                    if self.launch_mode != "timed":
+                        batch.set_persistent(self.launch_mode == "persistent")
                     sizes = tuple(sorted({a["req"].n for a in grouped}))
                     if sizes in self.tiles:
                         variants, mode = self.tiles[sizes]
                         batch.set_tiles(variants)
-                        if mode is not None:
+                        if mode is not None and self.launch_mode == "timed":
                             batch.set_persistent(mode == 2)
                         else:
                             tuned_now = sizes  # the launch mode is still to be timed

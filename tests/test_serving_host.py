@@ -48,7 +48,7 @@ class FakeBatch:
         pass
 
     def set_persistent(self, on):
-        pass
+        EVENTS.append(("persistent", on))
 
     def step(self, k, sync=True):
         assert not self.closed
@@ -108,3 +108,16 @@ def test_serving_admission_budget(fake_backend):
     out = srv.run(reqs, realtime=False)
     assert out["max_active"] == 2
     assert len(out["results"]) == 6
+
+
+@pytest.mark.parametrize("mode,expect", [("per_kernel", False), ("persistent", True)])
+def test_serving_forced_launch_mode(fake_backend, mode, expect):
+    reqs = serving.make_stream(6, rate=0.0, seed=5, sizes=(8, 16), steps=(5, 12))
+    srv = serving.Server(mixed=True, hbm_budget=1 << 40, max_slots=4, round_steps=4, solo_min=1000,
+                         launch_mode=mode)
+    out = srv.run(reqs, realtime=False)
+    assert len(out["results"]) == 6
+    calls = [e[1] for e in EVENTS if e[0] == "persistent"]
+    assert calls and all(c is expect for c in calls)
+    with pytest.raises(ValueError):
+        serving.Server(mixed=True, hbm_budget=1 << 40, launch_mode="fastest")

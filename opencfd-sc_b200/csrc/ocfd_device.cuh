@@ -86,6 +86,55 @@ struct Phys {
 // sums; the reference's order (h1(i) - h1(i-1) + h2(i) - h2(i-1)) is kept by
 // the strict build.
 #define OCFD_FV_SUMMED OCFD_FEWER_DIVS
+// Production build: the 5 face-flux components of a face are stored as a
+// 4-component record (32 bytes FP64, 16 bytes FP32; one 256-/128-bit access)
+// followed, after all records, by the 5th component as its own array: element
+// (face f, component m < 4) at 4 f + m, component 4 at 4 nfaces + f.  The
+// strict build keeps one array per component (f + m nfaces).
+#ifndef OCFD_HF_REC
+#define OCFD_HF_REC OCFD_FEWER_DIVS
+#endif
+
+// 4 consecutive values (32-byte aligned FP64 / 16-byte aligned FP32): one
+// 256-bit (sm_100) or 128-bit global access.
+__device__ __forceinline__ void rec4_store(double* p, double a, double b, double c, double d) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+__device__ __forceinline__ void rec4_store(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+// read-only within the launch, or written by other blocks of the same launch
+// before a counted wait (the persistent batched stage: no block reads a line of
+// these arrays before the wait, so no stale copy can sit in its L1)
+__device__ __forceinline__ void rec4_load(const double* p, double* o) {
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]) : "l"(p));
+}
+__device__ __forceinline__ void rec4_load(const float* p, float* o) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+  o[0] = t.x;
+  o[1] = t.y;
+  o[2] = t.z;
+  o[3] = t.w;
+}
+// the 5 face-flux components of face f (record layout or one array per component)
+template <typename R>
+__device__ __forceinline__ void hf_store5(R* out, long long f, long long nf, const R* v) {
+#if OCFD_HF_REC
+  rec4_store(out + 4 * f, v[0], v[1], v[2], v[3]);
+  out[4 * nf + f] = v[4];
+#else
+#pragma unroll
+  for (int m = 0; m < 5; m++) out[f + m * nf] = v[m];
+#endif
+}
+// offset of component m of face f
+__host__ __device__ __forceinline__ long long hf_at(long long f, long long nf, int m) {
+#if OCFD_HF_REC
+  return m < 4 ? 4 * f + m : 4 * nf + f;
+#else
+  return f + m * nf;
+#endif
+}
 
 // Metric m at haloed index c, or the constant +0.0 when the array holds only zeros.
 template <typename R, typename S>

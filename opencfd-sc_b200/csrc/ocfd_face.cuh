@@ -798,7 +798,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
             h2 = schemeM<SCHEME>(wv + 3, U, ihy);
           }
           if (OCFD_FV_SUMMED) {
-            out[fo + (long long)m * a.fs] = h1 + h2;
+            out[hf_at(fo, a.fs, m)] = h1 + h2;
           } else {
             out[fo + (long long)m * a.fs] = h1;
             out[fo + (long long)(5 + m) * a.fs] = h2;
@@ -815,7 +815,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
           for (int q = 0; q < 8; q++) wv[q] = W(5 + m, q);
           const R h2 = nc_flux2_bnd<SCHEME>(wv + 3, U, g, nn, ihy, ph, DIR);
           if (OCFD_FV_SUMMED) {
-            out[fo + (long long)m * a.fs] = h1 + h2;
+            out[hf_at(fo, a.fs, m)] = h1 + h2;
           } else {
             out[fo + (long long)m * a.fs] = h1;
             out[fo + (long long)(5 + m) * a.fs] = h2;
@@ -1239,8 +1239,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
 #endif
       }
     }
-#pragma unroll
-    for (int m = 0; m < 5; m++) out[fo + (long long)m * a.fs] = hh[m];
+    hf_store5(out, fo, a.fs, hh);
   }
   if constexpr (DEFER) {
     __syncthreads();
@@ -1266,8 +1265,7 @@ __device__ __forceinline__ void face_body(const FaceArgs<S>& a, const int bx, co
       for (int r = 0; r < 5; r++) h0[r] = xadd(dP[r], dM[r]);
       R hh[5];
       dcb.back(h0, hh, R(ph.inv_gm1));
-#pragma unroll
-      for (int m = 0; m < 5; m++) out[dfo + (long long)m * a.fs] = hh[m];
+      hf_store5(out, dfo, a.fs, hh);
     }
   }
 }

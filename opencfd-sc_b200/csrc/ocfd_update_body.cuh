@@ -13,8 +13,9 @@
 // Minimum resident blocks per SM requested for the viscous-gradient and
 // stage-tail kernels (both memory-latency bound: more resident warps keep
 // more loads in flight, at the price of registers).  Measured best on B200 at
-// 256^3: FP64 tail 5 (with the 256-bit viscous-flux loads; 3 / 4 / 6 blocks:
-// 3.93 / 3.63 / 4.37 against 3.60 ms per step), FP32 tail 5 (with the
+// 256^3: FP64 tail 4 with the face-flux records (3.52 against 3.75 ms per step
+// at 5 blocks; with one array per face-flux component 5 was best: 3 / 4 / 6
+// blocks 3.93 / 3.63 / 4.37 against 3.60 ms), FP32 tail 5 (with the
 // interleaved viscous fluxes; 5 and 6 before), FP64 viscous 4 (3 / 5 / 6
 // blocks: 3.48 / 4.04 / 5.49 against 2.76 ms per step: fewer warps expose the
 // stencil-load latency, more spill), FP32 viscous 6 (against 2-3 blocks with
@@ -26,7 +27,7 @@
 #define OCFD_VISC32_MINB 6
 #endif
 #ifndef OCFD_TAIL64_MINB
-#define OCFD_TAIL64_MINB 5
+#define OCFD_TAIL64_MINB 4
 #endif
 #ifndef OCFD_TAIL32_MINB
 #define OCFD_TAIL32_MINB 5
@@ -302,6 +303,33 @@ __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k
     f0[d] = (IX)G.face(d, lm, i, j, k);
   }
   const R ajac = R(a.ajac[G.ih(i, j, k)]);
+#if OCFD_HF_REC
+  // record layout: the four leading components of a face in one 256-bit
+  // (FP64) / 128-bit (FP32) load; the same operations, direction by direction
+  {
+    R acc[5];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const R* H = a.hf[d];
+      const IX fs = (IX)a.fs[d];
+      R h1[5], h0[5];
+      rec4_load(H + 4 * f1[d], h1);
+      rec4_load(H + 4 * f0[d], h0);
+      h1[4] = H[4 * fs + f1[d]];
+      h0[4] = H[4 * fs + f0[d]];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        const R dd = (h1[m] - h0[m]) * R(a.h_1[d]);
+        if (d == 0)
+          acc[m] = dd;
+        else if (d == 1)
+          acc[m] = acc[m] + dd;
+        else
+          du[m] = -(acc[m] + dd) * ajac;
+      }
+    }
+  }
+#else
 #pragma unroll
   for (int m = 0; m < 5; m++) {
     R dd[3];
@@ -319,6 +347,7 @@ __device__ __forceinline__ void inv_div(const UpdArgs<R>& a, int i, int j, int k
     acc = acc + dd[1];
     du[m] = -(acc + dd[2]) * ajac;
   }
+#endif
   if (a.ph.if_mass_force == 1) {
     const long long c = G.ih(i, j, k);
     const R d = R(a.pd[c]), u = R(a.pu[c]), v = R(a.pv[c]), w = R(a.pw[c]);

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad(ViscArgs<R, S
   visc_grad_body<R, S, AXS>(a, bx, by, bz);
 }
 template <typename R, typename S>
-__global__ void __launch_bounds__(256, OCFD_VISC_MINB) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
+__global__ void __launch_bounds__(256, OCFD_VISCB_MINB) k_visc_grad_batch(BatchTab<ViscArgs<R, S>> b) {
   __shared__ __align__(16) ViscArgs<R, S> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused(UpdArgs<R> a, Sla
   fused_body<CHAR, VISC, FUSEBC, R, IX>(a, bx, by, bz);
 }
 template <bool CHAR, bool VISC, bool FUSEBC, typename R, typename IX = long long>
-__global__ void __launch_bounds__(256, OCFD_TAIL_MINB) k_fused_batch(BatchTab<UpdArgs<R>> b) {
+__global__ void __launch_bounds__(256, OCFD_TAILB_MINB) k_fused_batch(BatchTab<UpdArgs<R>> b) {
   __shared__ __align__(16) UpdArgs<R> sa;
   int bx, by, bz;
   const int q = batch_locate(b, blockIdx.x, bx, by, bz);

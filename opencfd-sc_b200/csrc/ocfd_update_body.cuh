@@ -39,6 +39,17 @@
 #define OCFD_V256 1
 #endif
 #define OCFD_TAIL_MINB (sizeof(R) == 8 ? OCFD_TAIL64_MINB : OCFD_TAIL32_MINB)
+// the batched launches (arguments from shared memory, the member search):
+// the FP32 tail at 4 blocks (5 spilled about 600 bytes; 4 measured 0.5-1.5%
+// faster over the served member sets), the viscous kernel as the single one
+#ifndef OCFD_VISCB32_MINB
+#define OCFD_VISCB32_MINB OCFD_VISC32_MINB
+#endif
+#ifndef OCFD_TAILB32_MINB
+#define OCFD_TAILB32_MINB 4
+#endif
+#define OCFD_VISCB_MINB (sizeof(R) == 8 ? OCFD_VISC64_MINB : OCFD_VISCB32_MINB)
+#define OCFD_TAILB_MINB (sizeof(R) == 8 ? OCFD_TAIL64_MINB : OCFD_TAILB32_MINB)
 
 namespace ocfd {
 
